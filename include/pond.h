@@ -1,0 +1,145 @@
+/*
+ * pond.h -- C ABI of the B200 (sm_100a) Particles-on-Demand step library
+ * (lbmpond_b200/libpond_b200.so).
+ *
+ * Drop-in boundary for the reference's step entry points (engrab6/lbmPonD):
+ *
+ *   reference (global state, exit() on error)        this ABI (explicit context, status codes)
+ *   ------------------------------------------------  ----------------------------------------
+ *   LBMParamsHost::set      lbm.cu:134-168           pond_params_default + pond_create
+ *   copy2dev(tables)        lbm.cu:201-250           pond_create (tables live in the library)
+ *   void init()             init.cu:109-128          pond_init (built-in initial conditions)
+ *   fill / Cell::set_base   init.cu:2-108,           pond_set_state (host arrays; f = NULL
+ *                           lbpack.cu:15-21            means set_base from rho, u, T)
+ *   void calcStep()         update.cu:86-142         pond_step (minus file I/O and printf)
+ *   calcTotMoments/diagn    update.cu:52-69,         pond_diagnostics
+ *                           diagn.cu:1-30
+ *   void drop(string*)      drop.cu:2-34             pond_get_fields / pond_get_state
+ *   LBMParamsHost::swapLS   structs.cuh:148          done inside pond_step
+ *
+ * Every function returns POND_OK (0) or a negative pond_status; none exits
+ * the process.  A context belongs to one device and one CUDA stream; calls on
+ * one context must not overlap from several threads, while separate contexts
+ * are independent.  Host arrays are float64 in the layout
+ *   f[q*N + n], rho[n], g[k*N + n] (k: 0,1,2 = u_x,u_y,u_z; 3 = T),
+ *   n = x + Nx*(y + Ny*z), populations in the reference's order (consts.h).
+ */
+#ifndef POND_H
+#define POND_H
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define POND_ABI_VERSION 1
+
+typedef enum {
+  POND_OK = 0,
+  POND_ERR_ARG = -1,          /* bad argument or parameter combination */
+  POND_ERR_CUDA = -2,         /* a CUDA runtime call failed (see pond_last_error_string) */
+  POND_ERR_NOMEM = -3,        /* device allocation failed */
+  POND_ERR_STATE = -4,        /* call out of order (e.g. step before init) */
+  POND_ERR_UNSUPPORTED = -5,  /* lattice / scheme / precision combination not built */
+  POND_ERR_NOT_CONVERGED = -6 /* reserved for callers that treat max_iter hits as errors */
+} pond_status;
+
+/* lattices: consts.h:6-12 picks one at compile time; here it is a parameter */
+enum { POND_D1Q5 = 0, POND_D3Q27 = 1, POND_D3Q125 = 2 };
+/* interpolation at the departure point (steps.cu:444-463 call sites) */
+enum {
+  POND_LAGR2 = 2, POND_LAGR3 = 3, POND_LAGR4 = 4, POND_LAGR5 = 5, /* propagate<N>, steps.cu:986 */
+  POND_FIXED3 = 6, /* quadratic, origin fixed at coord-1: PonDstepD3Q125 steps.cu:151 */
+  POND_TVD = 7,    /* flux-difference minmod form, steps.cu:118-124 with call site :447 */
+  POND_WENO5 = 8   /* propagateWENO<3,5>, steps.cu:774-825 */
+};
+/* boundaries per axis: periodic is the reference (steps.cu:1015-1017); mirror
+   is its disabled outflow reflection (steps.cu:1004-1013); clamp = zero gradient */
+enum { POND_BC_PERIODIC = 0, POND_BC_CLAMP = 1, POND_BC_MIRROR = 2 };
+/* arithmetic of populations, interpolation and collision; conserved-moment
+   sums and the convergence test are float64 in both */
+enum { POND_FP32 = 0, POND_FP64 = 1 };
+/* built-in initial conditions for pond_init (init.cu:2-108 keeps its library
+   of ICs as overwritten assignments; each is a separate choice here) */
+enum {
+  POND_IC_ACOUSTIC = 0,  /* small-amplitude isentropic wave, init.cu:43-50 (the shipped IC) */
+  POND_IC_SOD_X = 1,     /* planar Riemann problem along x */
+  POND_IC_SPHERE = 2,    /* spherical Riemann problem */
+  POND_IC_TGV = 3,       /* compressible Taylor-Green vortex, init.cu:54-65 */
+  POND_IC_UNIFORM = 4    /* rho, u, T constant */
+};
+
+/* LBMParams (structs.cuh:100-122) + PhysPars (:96-99) + the compile-time
+   switches of consts.h / params.h, as runtime fields */
+typedef struct {
+  int64_t Nx, Ny, Nz;
+  int lattice;
+  int interp;
+  int precision;
+  int bc[3];
+  double tau;      /* relaxation time; the step uses dtau = 1/tau */
+  double dt;       /* time advanced per step (bookkeeping, LBMParams::dt) */
+  double tol_abs;  /* isConv: |new-old| < tol_abs + tol_rel*|new| on u, T and every f */
+  double tol_rel;
+  int max_iter;    /* fixed-point iteration cap (steps.cu:422: 100) */
+  int device;      /* CUDA device ordinal */
+  int learned;     /* 1: start each node's iteration from the predictor's gauge */
+  int reserved[5];
+} pond_params;
+
+/* diagnostics of the last completed step (update.cu:124-135, diagn.cu:24-30) */
+typedef struct {
+  double mass;        /* sum rho */
+  double moment[3];   /* sum rho*u (the reference prints the x component) */
+  double enrg;        /* sum rho*(u.u + Dim*T)  (update.cu:67) */
+  double k;           /* sum 0.5|u|^2 dx dy dz/(8 pi^3), dx = 2pi/Nx (diagn.cu:18) */
+  int32_t niter_max;  /* LBMParams::NiterMax */
+  int32_t pad;
+  double niter_mean;
+  int64_t niter_sum;
+  int64_t nonconverged; /* nodes that reached max_iter without meeting the tolerance */
+  int64_t istep;
+  double curtime;
+} pond_diag;
+
+typedef struct pond_ctx pond_ctx;
+
+int pond_abi_version(void);
+const char* pond_status_string(int status);
+/* message of the last failing call on this thread */
+const char* pond_last_error_string(void);
+
+int pond_params_default(int lattice, pond_params* out);
+int pond_create(const pond_params* params, pond_ctx** out);
+int pond_destroy(pond_ctx* ctx);
+int pond_get_params(const pond_ctx* ctx, pond_params* out);
+int pond_q(int lattice);
+
+/* ic_params: ACOUSTIC {T0, amplitude, gamma}; SOD_X {x0, rhoL, uL, TL, rhoR, uR, TR};
+   SPHERE {cx, cy, cz, radius, rho_in, T_in, rho_out, T_out};
+   TGV {U0, T0, rho0, gamma}; UNIFORM {rho, ux, uy, uz, T} */
+int pond_init(pond_ctx* ctx, int ic, const double* ic_params, int n_params);
+/* upload a state from host memory; f == NULL applies set_base (f_i = w_i*rho) */
+int pond_set_state(pond_ctx* ctx, const double* f, const double* rho, const double* g);
+int pond_get_state(pond_ctx* ctx, double* f, double* rho, double* g);
+/* any pointer may be NULL; each receives N values */
+int pond_get_fields(pond_ctx* ctx, double* rho, double* ux, double* uy, double* uz, double* T);
+/* advance nsteps steps (calcStep without drop/diagnostics printing) */
+int pond_step(pond_ctx* ctx, int nsteps);
+int pond_diagnostics(pond_ctx* ctx, pond_diag* out);
+/* per-node iteration counts of the last step (int32[N]); needs pond_keep_niter(ctx, 1) before the step */
+int pond_keep_niter(pond_ctx* ctx, int on);
+int pond_get_niter(pond_ctx* ctx, int32_t* niter);
+
+/* the context's CUDA stream (a cudaStream_t) */
+void* pond_stream(pond_ctx* ctx);
+/* device pointers of the current state (for zero-copy callers on the same device):
+   f[Q*N], rho[N], g[4*N] in the context's precision (float or double) */
+int pond_device_state(pond_ctx* ctx, void** f, void** rho, void** g);
+/* synchronous device-time of the last pond_step call's step kernels, in ms */
+int pond_last_step_ms(pond_ctx* ctx, float* ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

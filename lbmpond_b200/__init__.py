@@ -1,0 +1,194 @@
+"""B200-native Particles-on-Demand (PonD) lattice-Boltzmann step.
+
+Host-side mirror of the reference's step interface (engrab6/lbmPonD):
+
+    reference                          here
+    ---------------------------------  -----------------------------------
+    init()           init.cu:109       Solver.init(ic, ...)
+    calcStep()       update.cu:86      Solver.step(n) / Solver.calcStep()
+    diagnostics()    diagn.cu:24       Solver.diagnostics()
+    drop(&dir)       drop.cu:2         Solver.drop(dir)  (.arr files)
+
+All arithmetic runs in the CUDA library libpond_b200.so (sm_100a) behind the
+C ABI of include/pond.h; this module only marshals arguments.  There is no
+CPU fallback: constructing a Solver without the built library or a CUDA
+device raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import _lib
+from ._lib import (BC_CLAMP, BC_MIRROR, BC_PERIODIC, D1Q5, D3Q27, D3Q125, FIXED3, FP32, FP64, IC_ACOUSTIC,
+                   IC_SOD_X, IC_SPHERE, IC_TGV, IC_UNIFORM, LAGR2, LAGR3, LAGR4, LAGR5, TVD, WENO5, PondError)
+
+__all__ = ["Solver", "PondError", "lattice_q", "D1Q5", "D3Q27", "D3Q125", "LAGR2", "LAGR3", "LAGR4", "LAGR5",
+           "FIXED3", "TVD", "WENO5", "BC_PERIODIC", "BC_CLAMP", "BC_MIRROR", "FP32", "FP64", "IC_ACOUSTIC",
+           "IC_SOD_X", "IC_SPHERE", "IC_TGV", "IC_UNIFORM", "write_arr", "read_arr"]
+
+_LATTICES = {"D1Q5": D1Q5, "D3Q27": D3Q27, "D3Q125": D3Q125}
+_BCS = {"periodic": BC_PERIODIC, "clamp": BC_CLAMP, "zero_gradient": BC_CLAMP, "mirror": BC_MIRROR}
+_ICS = {"acoustic": IC_ACOUSTIC, "sod": IC_SOD_X, "sphere": IC_SPHERE, "tgv": IC_TGV, "uniform": IC_UNIFORM}
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if a is not None else None
+
+
+def lattice_q(lattice) -> int:
+    lat = _LATTICES.get(lattice, lattice)
+    return _lib.load().pond_q(int(lat))
+
+
+class Solver:
+    """One PonD simulation context on one GPU (wraps pond_ctx)."""
+
+    def __init__(self, lattice="D3Q27", shape=(32, 32, 32), interp=None, precision="fp32", tau=0.9,
+                 tol_abs=None, tol_rel=None, max_iter=100, bc=("periodic",) * 3, device=0, dt=1.0,
+                 learned=False):
+        L = _lib.load()
+        lat = _LATTICES.get(lattice, lattice)
+        p = _lib.PondParams()
+        _lib.check(L.pond_params_default(int(lat), ctypes.byref(p)))
+        p.Nx, p.Ny, p.Nz = (int(v) for v in shape)
+        if interp is not None:
+            p.interp = int(interp)
+        p.precision = {"fp32": FP32, "fp64": FP64}.get(precision, precision)
+        if p.precision == FP64:  # the reference's USE_DOUBLE tolerances (steps.cu:62-63)
+            p.tol_abs, p.tol_rel = 1e-12, 1e-10
+        if tol_abs is not None:
+            p.tol_abs = tol_abs
+        if tol_rel is not None:
+            p.tol_rel = tol_rel
+        p.tau = tau
+        p.dt = dt
+        p.max_iter = max_iter
+        p.device = device
+        p.learned = 1 if learned else 0
+        for a in range(3):
+            p.bc[a] = _BCS.get(bc[a], bc[a])
+        ctx = ctypes.c_void_p()
+        _lib.check(L.pond_create(ctypes.byref(p), ctypes.byref(ctx)))
+        self._L = L
+        self._ctx = ctx
+        self.params = p
+        self.lattice = int(lat)
+        self.shape = (int(p.Nx), int(p.Ny), int(p.Nz))
+        self.N = self.shape[0] * self.shape[1] * self.shape[2]
+        self.Q = L.pond_q(self.lattice)
+
+    # -- lifetime
+    def close(self):
+        if getattr(self, "_ctx", None):
+            self._L.pond_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._ctx
+
+    # -- reference entry points
+    def init(self, ic="acoustic", *params):
+        """Built-in initial condition + set_base on both buffers (init.cu:109-128)."""
+        code = _ICS.get(ic, ic)
+        arr = np.ascontiguousarray(params, dtype=np.float64) if params else None
+        _lib.check(self._L.pond_init(self._ctx, int(code), _dp(arr), len(params)))
+
+    def set_state(self, rho, g, f=None):
+        rho = np.ascontiguousarray(rho, dtype=np.float64).reshape(self.N)
+        g = np.ascontiguousarray(g, dtype=np.float64).reshape(4, self.N)
+        if f is not None:
+            f = np.ascontiguousarray(f, dtype=np.float64).reshape(self.Q, self.N)
+        _lib.check(self._L.pond_set_state(self._ctx, _dp(f), _dp(rho), _dp(g)))
+
+    def get_state(self):
+        f = np.empty((self.Q, self.N)); rho = np.empty(self.N); g = np.empty((4, self.N))
+        _lib.check(self._L.pond_get_state(self._ctx, _dp(f), _dp(rho), _dp(g)))
+        return f, rho, g
+
+    def fields(self):
+        out = [np.empty(self.N) for _ in range(5)]
+        _lib.check(self._L.pond_get_fields(self._ctx, *[_dp(a) for a in out]))
+        return dict(zip(("rho", "ux", "uy", "uz", "T"), out))
+
+    def step(self, n=1):
+        _lib.check(self._L.pond_step(self._ctx, int(n)))
+
+    calcStep = step
+
+    def diagnostics(self) -> dict:
+        d = _lib.PondDiag()
+        _lib.check(self._L.pond_diagnostics(self._ctx, ctypes.byref(d)))
+        return {"mass": d.mass, "moment": tuple(d.moment), "enrg": d.enrg, "k": d.k, "niter_max": d.niter_max,
+                "niter_mean": d.niter_mean, "niter_sum": d.niter_sum, "nonconverged": d.nonconverged,
+                "istep": d.istep, "curtime": d.curtime}
+
+    def keep_niter(self, on=True):
+        _lib.check(self._L.pond_keep_niter(self._ctx, 1 if on else 0))
+
+    def niter(self):
+        out = np.empty(self.N, dtype=np.int32)
+        _lib.check(self._L.pond_get_niter(self._ctx, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))))
+        return out
+
+    def last_step_ms(self) -> float:
+        ms = ctypes.c_float()
+        _lib.check(self._L.pond_last_step_ms(self._ctx, ctypes.byref(ms)))
+        return float(ms.value)
+
+    def stream(self) -> int:
+        return int(self._L.pond_stream(self._ctx) or 0)
+
+    def device_state(self):
+        f, r, g = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+        _lib.check(self._L.pond_device_state(self._ctx, ctypes.byref(f), ctypes.byref(r), ctypes.byref(g)))
+        return f.value, r.value, g.value
+
+    def drop(self, directory: str):
+        """Write Rho/Vx/Vy/Vz/T_%07d.arr for the current step (drop.cu:2-34)."""
+        fl = self.fields()
+        istep = self.diagnostics()["istep"]
+        os.makedirs(directory, exist_ok=True)
+        names = {"Rho": "rho", "Vx": "ux", "Vy": "uy", "Vz": "uz", "T": "T"}
+        paths = []
+        for prefix, key in names.items():
+            path = os.path.join(directory, f"{prefix}_{istep:07d}.arr")
+            write_arr(path, fl[key], self.shape)
+            paths.append(path)
+        return paths
+
+
+def write_arr(path: str, data, shape):
+    """The reference's .arr layout (drop.cu:12-30): int32 comment length (0),
+    int32 dim (3), int32 sizeof(value) (8), int32 Nx, Ny, Nz, then float64
+    values with x fastest."""
+    nx, ny, nz = shape
+    with open(path, "wb") as fp:
+        np.array([0, 3, 8, nx, ny, nz], dtype=np.int32).tofile(fp)
+        np.ascontiguousarray(data, dtype=np.float64).reshape(nx * ny * nz).tofile(fp)
+
+
+def read_arr(path: str):
+    with open(path, "rb") as fp:
+        clen = int(np.fromfile(fp, dtype=np.int32, count=1)[0])
+        if clen:
+            fp.read(clen)
+        dim, size, nx, ny, nz = (int(v) for v in np.fromfile(fp, dtype=np.int32, count=5))
+        dt = {8: np.float64, 4: np.float32}[size]
+        data = np.fromfile(fp, dtype=dt, count=nx * ny * nz)
+    return data, (nx, ny, nz)

@@ -1,0 +1,51 @@
+// Host-side internals shared by the library's translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "pond_common.cuh"
+
+struct pond_ctx {
+  pond_params p;
+  int Q = 0;
+  long long N = 0;
+  size_t elem = 4;           // bytes per stored value (float or double)
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // double-buffered SoA state: f[Q][N], rho[N], g[4][N]; cur is the latest
+  void* f[2] = {nullptr, nullptr};
+  void* rho[2] = {nullptr, nullptr};
+  void* g[2] = {nullptr, nullptr};
+  int cur = 0;
+  pond::StepSums* d_sums = nullptr;
+  pond::StepSums* h_sums = nullptr;  // pinned
+  bool have_sums = false;
+  int* niter = nullptr;
+  bool keep_niter = false;
+  float* guess = nullptr;  // [4][N] predicted starting gauge (learned path)
+  bool guess_ready = false;
+  void* predictor = nullptr;  // learned-gauge network bound to this context
+  bool initialized = false;
+  long long istep = 0;
+  double curtime = 0;
+  void* staging = nullptr;  // pinned host staging for conversions
+  size_t staging_bytes = 0;
+};
+
+namespace pond {
+int set_error(int status, const char* fmt, ...);
+int cuda_fail(cudaError_t e, const char* what);
+int lattice_q(int lattice);
+double lattice_weight_host(int lattice, int ref_index);
+double lattice_tlat(int lattice);
+double lattice_dim(int lattice);
+
+int ctx_alloc(pond_ctx* c);
+void ctx_free(pond_ctx* c);
+// float64 host array -> device array of the context's precision (and back)
+int upload(pond_ctx* c, const double* src, size_t count, void* dst);
+int download(pond_ctx* c, const void* src, size_t count, double* dst);
+int launch_step(pond_ctx* c);
+int state_sums(pond_ctx* c, pond_diag* out);
+// learned path: run the bound predictor on the current state into c->guess
+int run_predictor(pond_ctx* c);
+}  // namespace pond

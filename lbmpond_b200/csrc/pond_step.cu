@@ -1,0 +1,226 @@
+// Step dispatch, buffer management and host<->device conversion.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <vector>
+
+#include "pond_internal.h"
+#include "pond_step_1d.cuh"
+#include "pond_step_d3q125.cuh"
+#include "pond_step_point.cuh"
+
+namespace pond {
+
+int ctx_alloc(pond_ctx* c) {
+  cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
+  if ((e = cudaEventCreate(&c->ev0)) != cudaSuccess) return cuda_fail(e, "cudaEventCreate");
+  if ((e = cudaEventCreate(&c->ev1)) != cudaSuccess) return cuda_fail(e, "cudaEventCreate");
+  const size_t N = (size_t)c->N;
+  for (int b = 0; b < 2; b++) {
+    if (cudaMalloc(&c->f[b], (size_t)c->Q * N * c->elem) != cudaSuccess ||
+        cudaMalloc(&c->rho[b], N * c->elem) != cudaSuccess || cudaMalloc(&c->g[b], 4 * N * c->elem) != cudaSuccess) {
+      cudaGetLastError();
+      return set_error(POND_ERR_NOMEM, "state buffers (%zu bytes each)", (size_t)(c->Q + 5) * N * c->elem);
+    }
+  }
+  if (cudaMalloc(&c->d_sums, sizeof(StepSums)) != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(POND_ERR_NOMEM, "step sums");
+  }
+  if ((e = cudaMallocHost(&c->h_sums, sizeof(StepSums))) != cudaSuccess) return cuda_fail(e, "cudaMallocHost");
+  std::memset(c->h_sums, 0, sizeof(StepSums));
+  return POND_OK;
+}
+
+void ctx_free(pond_ctx* c) {
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (int b = 0; b < 2; b++) {
+    cudaFree(c->f[b]); cudaFree(c->rho[b]); cudaFree(c->g[b]);
+    c->f[b] = c->rho[b] = c->g[b] = nullptr;
+  }
+  cudaFree(c->d_sums); c->d_sums = nullptr;
+  cudaFree(c->niter); c->niter = nullptr;
+  cudaFree(c->guess); c->guess = nullptr;
+  if (c->h_sums) cudaFreeHost(c->h_sums);
+  c->h_sums = nullptr;
+  if (c->staging) cudaFreeHost(c->staging);
+  c->staging = nullptr;
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  c->ev0 = c->ev1 = nullptr;
+  c->stream = nullptr;
+}
+
+static int ensure_staging(pond_ctx* c, size_t bytes) {
+  if (c->staging_bytes >= bytes) return POND_OK;
+  if (c->staging) cudaFreeHost(c->staging);
+  c->staging = nullptr;
+  c->staging_bytes = 0;
+  cudaError_t e = cudaMallocHost(&c->staging, bytes);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMallocHost staging");
+  c->staging_bytes = bytes;
+  return POND_OK;
+}
+
+static constexpr size_t CHUNK = size_t(1) << 22;  // elements per staged copy
+
+int upload(pond_ctx* c, const double* src, size_t count, void* dst) {
+  if (c->elem == 8) {
+    cudaError_t e = cudaMemcpyAsync(dst, src, count * 8, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    return e == cudaSuccess ? POND_OK : cuda_fail(e, "upload");
+  }
+  int st = ensure_staging(c, CHUNK * 4);
+  if (st != POND_OK) return st;
+  float* stg = (float*)c->staging;
+  for (size_t o = 0; o < count; o += CHUNK) {
+    const size_t n = count - o < CHUNK ? count - o : CHUNK;
+    for (size_t i = 0; i < n; i++) stg[i] = (float)src[o + i];
+    cudaError_t e = cudaMemcpyAsync((float*)dst + o, stg, n * 4, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "upload");
+  }
+  return POND_OK;
+}
+
+int download(pond_ctx* c, const void* src, size_t count, double* dst) {
+  if (c->elem == 8) {
+    cudaError_t e = cudaMemcpyAsync(dst, src, count * 8, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    return e == cudaSuccess ? POND_OK : cuda_fail(e, "download");
+  }
+  int st = ensure_staging(c, CHUNK * 4);
+  if (st != POND_OK) return st;
+  float* stg = (float*)c->staging;
+  for (size_t o = 0; o < count; o += CHUNK) {
+    const size_t n = count - o < CHUNK ? count - o : CHUNK;
+    cudaError_t e = cudaMemcpyAsync(stg, (const float*)src + o, n * 4, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "download");
+    for (size_t i = 0; i < n; i++) dst[o + i] = stg[i];
+  }
+  return POND_OK;
+}
+
+// ---------------------------------------------------------------- sums of a state
+template <typename R>
+__global__ void state_sums_kernel(const R* rho, const R* g, long long N, double dim, double kdx, StepSums* out) {
+  const long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  NodeSums ns = {0, 0, 0, 0, 0, 0, 0ull, 0ull, 0};
+  if (n < N) {
+    const double r = rho[n], u0 = g[n], u1 = g[N + n], u2 = g[2 * N + n], T = g[3 * N + n];
+    const double u2s = u0 * u0 + u1 * u1 + u2 * u2;
+    ns.mass = r; ns.m0 = r * u0; ns.m1 = r * u1; ns.m2 = r * u2;
+    ns.enrg = r * (u2s + dim * T);
+    ns.k = kdx * u2s;
+  }
+  reduce_and_commit(ns, out);
+}
+
+static double kdx_of(const pond_ctx* c) {
+  const double PI = 3.14159265358979323846;
+  return 0.5 / (8 * PI * PI * PI) * (2 * PI / c->p.Nx) * (2 * PI / c->p.Ny) * (2 * PI / c->p.Nz);
+}
+
+int state_sums(pond_ctx* c, pond_diag* out) {
+  cudaError_t e = cudaMemsetAsync(c->d_sums, 0, sizeof(StepSums), c->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "memset");
+  const int th = 256;
+  const unsigned blocks = (unsigned)((c->N + th - 1) / th);
+  const double dim = lattice_dim(c->p.lattice);
+  if (c->elem == 8)
+    state_sums_kernel<double><<<blocks, th, 0, c->stream>>>((const double*)c->rho[c->cur], (const double*)c->g[c->cur],
+                                                            c->N, dim, kdx_of(c), c->d_sums);
+  else
+    state_sums_kernel<float><<<blocks, th, 0, c->stream>>>((const float*)c->rho[c->cur], (const float*)c->g[c->cur],
+                                                           c->N, dim, kdx_of(c), c->d_sums);
+  StepSums s;
+  e = cudaMemcpyAsync(&s, c->d_sums, sizeof(s), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "state sums");
+  out->mass = s.mass;
+  out->moment[0] = s.mom[0]; out->moment[1] = s.mom[1]; out->moment[2] = s.mom[2];
+  out->enrg = s.enrg;
+  out->k = s.k;
+  return POND_OK;
+}
+
+// ---------------------------------------------------------------- dispatch
+template <int LAT, int N, typename R> static void launch_point(const StepArgs<R>& a, cudaStream_t s) {
+  if (Lattice<LAT>::D == 1) {
+    dim3 blk(128, 1, 1), grd((a.nx + 127) / 128, a.ny, a.nz);
+    pull_point_kernel<LAT, N, R><<<grd, blk, 0, s>>>(a);
+  } else {
+    dim3 blk(32, 4, 1), grd((a.nx + 31) / 32, (a.ny + 3) / 4, a.nz);
+    pull_point_kernel<LAT, N, R><<<grd, blk, 0, s>>>(a);
+  }
+}
+
+template <typename R> static int launch_typed(pond_ctx* c) {
+  StepArgs<R> a;
+  const int i = c->cur, o = 1 - c->cur;
+  a.f_in = (const R*)c->f[i]; a.rho_in = (const R*)c->rho[i]; a.g_in = (const R*)c->g[i];
+  a.f_out = (R*)c->f[o]; a.rho_out = (R*)c->rho[o]; a.g_out = (R*)c->g[o];
+  a.guess = c->p.learned ? c->guess : nullptr;
+  a.niter_out = c->keep_niter ? c->niter : nullptr;
+  a.sums = c->d_sums;
+  a.nx = (int)c->p.Nx; a.ny = (int)c->p.Ny; a.nz = (int)c->p.Nz;
+  a.N = c->N;
+  for (int k = 0; k < 3; k++) a.bc[k] = c->p.bc[k];
+  a.dtau = 1.0 / c->p.tau;
+  a.tol_abs = c->p.tol_abs; a.tol_rel = c->p.tol_rel;
+  a.max_iter = c->p.max_iter;
+  a.kdx = kdx_of(c);
+  cudaError_t e = cudaMemsetAsync(c->d_sums, 0, sizeof(StepSums), c->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "memset sums");
+  cudaStream_t s = c->stream;
+  switch (c->p.lattice) {
+    case POND_D1Q5:
+      switch (c->p.interp) {
+        case POND_LAGR2: launch_point<POND_D1Q5, 2, R>(a, s); break;
+        case POND_LAGR3: launch_point<POND_D1Q5, 3, R>(a, s); break;
+        case POND_LAGR4: launch_point<POND_D1Q5, 4, R>(a, s); break;
+        case POND_LAGR5: launch_point<POND_D1Q5, 5, R>(a, s); break;
+        case POND_TVD:
+          pull_1d_scheme_kernel<POND_TVD, R><<<(a.nx + 127) / 128, 128, 0, s>>>(a);
+          break;
+        case POND_WENO5:
+          pull_1d_scheme_kernel<POND_WENO5, R><<<(a.nx + 127) / 128, 128, 0, s>>>(a);
+          break;
+        default: return set_error(POND_ERR_UNSUPPORTED, "scheme");
+      }
+      break;
+    case POND_D3Q27:
+      switch (c->p.interp) {
+        case POND_LAGR2: launch_point<POND_D3Q27, 2, R>(a, s); break;
+        case POND_LAGR3: launch_point<POND_D3Q27, 3, R>(a, s); break;
+        case POND_LAGR4: launch_point<POND_D3Q27, 4, R>(a, s); break;
+        case POND_LAGR5: launch_point<POND_D3Q27, 5, R>(a, s); break;
+        default: return set_error(POND_ERR_UNSUPPORTED, "scheme");
+      }
+      break;
+    case POND_D3Q125: {
+      const size_t smem = sizeof(D125Smem<R>);
+      e = cudaFuncSetAttribute(pull_d3q125_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+      pull_d3q125_kernel<R><<<(unsigned)c->N, D125_THREADS, smem, s>>>(a);
+      break;
+    }
+    default: return set_error(POND_ERR_UNSUPPORTED, "lattice");
+  }
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "step kernel launch");
+  return POND_OK;
+}
+
+int launch_step(pond_ctx* c) {
+  if (c->p.learned) {
+    int st = run_predictor(c);
+    if (st != POND_OK) return st;
+  }
+  return c->elem == 8 ? launch_typed<double>(c) : launch_typed<float>(c);
+}
+
+}  // namespace pond

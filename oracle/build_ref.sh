@@ -1,0 +1,51 @@
+#!/usr/bin/env bash
+# Build the reference's own CUDA step kernels (engrab6/lbmPonD) for sm_100a,
+# driven by oracle/ref_main.cu.  TEST INFRASTRUCTURE ONLY: the binaries pin
+# the FP64 oracle against the reference and time the reference kernels on
+# the GPU; nothing in the product links them.
+#
+#   oracle/build_ref.sh <D1Q5|D3Q27|D3Q125> <double|float> <nx> <ny> <nz>
+#
+# The reference sources stay where they are (read-only); patched copies live
+# in a temporary directory and only the binary is written, into oracle/_ref/.
+# Patches (the lattice, precision and grid size are compile-time constants in
+# the reference):
+#   consts.h:7       the live lattice #define
+#   params.h:13      USE_DOUBLE -> USE_FLOAT for the float build
+#   params.h:160-161 cudaPointerAttributes::memoryType -> type (CUDA >= 11)
+#   structs.cuh:10-12 LSizeX/Y/Z (grid = LSize * brick(4,1,1))
+#   im2D.h           replaced by a stub: the GL/GLUT window code is not on
+#                    the step's path and no graphics stack exists here
+set -euo pipefail
+REF=${POND_REFERENCE_DIR:-/root/reference}
+HERE=$(cd "$(dirname "$0")" && pwd)
+OUT="$HERE/_ref"
+LAT=${1:?lattice}; PREC=${2:?precision}; NX=${3:?nx}; NY=${4:?ny}; NZ=${5:?nz}
+case "$LAT" in D1Q5|D3Q27|D3Q125) ;; *) echo "bad lattice $LAT" >&2; exit 2;; esac
+case "$PREC" in double|float) ;; *) echo "bad precision $PREC" >&2; exit 2;; esac
+if (( NX % 4 != 0 )); then echo "nx must be a multiple of 4 (brick.x)" >&2; exit 2; fi
+if [ ! -f "$REF/steps.cu" ]; then echo "reference sources not found at $REF" >&2; exit 3; fi
+NVCC=${NVCC:-nvcc}
+mkdir -p "$OUT"
+BIN="$OUT/ref_pond_${LAT}_${PREC}_${NX}x${NY}x${NZ}"
+TMP=$(mktemp -d /tmp/pond_ref.XXXXXX)
+trap 'rm -rf "$TMP"' EXIT
+cp "$REF"/*.cu "$REF"/*.cuh "$REF"/*.h "$REF"/*.hpp "$TMP"/
+sed -i "s/^ #define D1Q5\$/ #define ${LAT}/" "$TMP/consts.h"
+grep -q "^ #define ${LAT}\$" "$TMP/consts.h"
+sed -i "s/^const long int LSizeX=.*/const long int LSizeX=$((NX / 4));/; s/^const long int LSizeY=.*/const long int LSizeY=${NY};/; s/^const long int LSizeZ=.*/const long int LSizeZ=${NZ};/" "$TMP/structs.cuh"
+sed -i 's/ptrAt\.memoryType/ptrAt.type/g' "$TMP/params.h"
+if [ "$PREC" = float ]; then sed -i 's/^#define USE_DOUBLE$/#define USE_FLOAT/' "$TMP/params.h"; fi
+cat > "$TMP/im2D.h" <<'EOF'
+#ifndef IM2D_H
+#define IM2D_H
+struct image2D { void get_device(int, int) {} };
+#endif
+EOF
+FLAGS=(-gencode arch=compute_100a,code=sm_100a -O3 -rdc=true -I"$TMP" -Xcudafe --diag_suppress=declared_but_not_referenced -w)
+for f in update init lbpack diagn drop; do
+  "$NVCC" "${FLAGS[@]}" -c "$TMP/$f.cu" -o "$TMP/$f.o"
+done
+"$NVCC" "${FLAGS[@]}" -c "$HERE/ref_main.cu" -o "$TMP/ref_main.o"
+"$NVCC" -gencode arch=compute_100a,code=sm_100a -rdc=true "$TMP"/*.o -o "$BIN"
+echo "$BIN"

@@ -1,0 +1,67 @@
+/*
+ * FP64 CPU oracle for the Particles-on-Demand (PonD) pull step.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library restates, in plain C++ with OpenMP,
+ * the reference's per-node PonD step (engrab6/lbmPonD: steps.cu LBMpull /
+ * PonDstepD3Q125, structs.cuh Cell::transfer_gauge / calcMoments, consts.h
+ * lattice tables).  It is the checker for the CUDA path and the timed CPU
+ * baseline; the product library never links, loads or calls it.
+ *
+ * Layout of every state array (the same as the CUDA library's host view):
+ *   f[q * N + n]      populations, q < Q, n = x + nx*(y + ny*z)
+ *   rho[n]            density
+ *   g[k * N + n]      gauge: k = 0,1,2 -> u_x,u_y,u_z ; k = 3 -> T
+ * Population order is the reference's (consts.h e_host order).
+ */
+#ifndef POND_ORACLE_H
+#define POND_ORACLE_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { ORC_D1Q5 = 0, ORC_D3Q27 = 1, ORC_D3Q125 = 2 };
+/* interpolation schemes; numbers 2..5 are Lagrange orders (steps.cu:986 propagate<N>) */
+enum { ORC_LAGR2 = 2, ORC_LAGR3 = 3, ORC_LAGR4 = 4, ORC_LAGR5 = 5,
+       ORC_FIXED3 = 6,   /* quadratic, stencil origin fixed at coord-1 (steps.cu:151 PonDstepD3Q125) */
+       ORC_TVD = 7,      /* flux-difference minmod form (steps.cu:118 FluxTVDdif, call site :447) */
+       ORC_WENO5 = 8 };  /* propagateWENO<3,5> (steps.cu:774) */
+enum { ORC_BC_PERIODIC = 0, ORC_BC_CLAMP = 1, ORC_BC_MIRROR = 2 };
+
+typedef struct {
+  int lattice;
+  int interp;
+  int64_t nx, ny, nz;
+  int bc[3];          /* per axis */
+  double tau;         /* BGK relaxation time; dtau = 1/tau (structs.cuh:98) */
+  double tol_abs;     /* isConv absolute tolerance (steps.cu:62) */
+  double tol_rel;     /* isConv relative tolerance (steps.cu:63) */
+  int max_iter;       /* iteration cap (steps.cu:422) */
+  int nthreads;       /* 0 = OpenMP default */
+} orc_params;
+
+int    orc_q(int lattice);
+/* xi[3*Q] real lattice directions (ef, or e for D3Q27), e[3*Q] integer
+   directions, w[Q] weights, out[0]=TLat, out[1]=Dim */
+int    orc_tables(int lattice, double* xi, int* e, double* w, double* tlat_dim);
+/* reference-order reverse maps per axis (consts.h / lbm.cu:206-244) */
+int    orc_reverse(int lattice, int* rev_x, int* rev_y, int* rev_z);
+void   orc_set_base(int lattice, double rho, const double* uT, double* f);
+double orc_transfer_gauge(int lattice, const double* f, const double* uT_src,
+                          const double* uT_dst, int inew);
+void   orc_calc_moments(int lattice, const double* f, const double* vi,
+                        double* rho, double* uT);
+double orc_lagr_pol(int n, int ix, int iy, int iz, double sx, double sy, double sz);
+/* one pull step; guess (4*N, optional) replaces each node's starting gauge;
+   niter (N, optional) receives each node's iteration count.
+   Returns the number of nodes that hit max_iter without converging. */
+int64_t orc_step(const orc_params* p,
+                 const double* f_in, const double* rho_in, const double* g_in,
+                 const double* guess,
+                 double* f_out, double* rho_out, double* g_out, int* niter);
+int    orc_max_threads(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,154 @@
+"""GPU parity of the CUDA step (through the C ABI) with the FP64 oracle.
+
+float64 runs must agree with the oracle to rounding plus the iteration
+tolerance; float32 runs (float32 populations and interpolation, float64
+moments and convergence test) must agree to float32 level.  Tolerances:
+
+  FP64: |d| <= 1e-9 * scale for f, rho, T; 1e-9 * sqrt(T) for u
+  FP32: |d| <= 3e-5 * scale for f, rho, T; 3e-5 * sqrt(T) for u
+"""
+import numpy as np
+import pytest
+
+from tests.states import perturbed_populations, smooth_state, sod_state
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp64": 1e-9, "fp32": 3e-5}
+
+
+def _state(orc, lat, shape, kind, seed):
+    dim = 1 if lat == 0 else 3
+    if kind == "sod":
+        rho, g = sod_state(shape[0])
+    else:
+        rho, g = smooth_state(shape, dim, seed=seed, modes=1, du=0.03)
+    f = perturbed_populations(orc, lat, rho, g, seed=seed, eps=0.01)
+    return orc.State(f, rho, g)
+
+
+def _compare(st_gpu, st_ref, tol, what=""):
+    f, rho, g = st_gpu
+    T = st_ref.g[3]
+    cs = np.sqrt(np.abs(T).max())
+    err = {
+        "f": np.abs(f - st_ref.f).max() / np.abs(st_ref.f).max(),
+        "rho": np.abs(rho - st_ref.rho).max() / np.abs(st_ref.rho).max(),
+        "u": np.abs(g[:3] - st_ref.g[:3]).max() / cs,
+        "T": np.abs(g[3] - T).max() / np.abs(T).max(),
+    }
+    bad = {k: v for k, v in err.items() if not v <= tol}
+    assert not bad, f"{what}: {err}"
+    return err
+
+
+def run_pair(orc, pond, lat, shape, interp, precision, tau=0.8, nsteps=2, kind="smooth", seed=0, bc=(0, 0, 0),
+             max_iter=100):
+    st = _state(orc, lat, shape, kind, seed)
+    s = pond.Solver(lattice=lat, shape=shape, interp=interp, precision=precision, tau=tau, bc=bc, max_iter=max_iter)
+    try:
+        s.set_state(st.rho, st.g, f=st.f)
+        ref = st
+        for _ in range(nsteps):
+            s.step(1)
+            ref, niter, nc = orc.step(ref, lat, shape, interp=interp, tau=tau, bc=bc, max_iter=max_iter)
+        out = s.get_state()
+        d = s.diagnostics()
+    finally:
+        s.close()
+    return out, ref, niter, nc, d
+
+
+CASES = [
+    # lattice, shape, interp
+    (0, (128, 1, 1), 4),
+    (0, (97, 1, 1), 4),   # ragged: not a multiple of the block
+    (0, (64, 1, 1), 2),
+    (0, (64, 1, 1), 3),
+    (0, (64, 1, 1), 5),
+    (0, (128, 1, 1), 7),  # TVD
+    (0, (128, 1, 1), 8),  # WENO5
+    (1, (8, 8, 8), 4),
+    (1, (9, 7, 5), 4),    # ragged in every axis
+    (1, (8, 6, 4), 3),
+    (1, (6, 6, 6), 2),
+    (1, (6, 5, 6), 5),
+    (2, (5, 4, 4), 6),
+]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("lat,shape,interp", CASES)
+def test_step_matches_oracle(orc, pond, lat, shape, interp, precision):
+    out, ref, niter, nc, d = run_pair(orc, pond, lat, shape, interp, precision)
+    _compare(out, ref, TOL[precision], f"lat={lat} shape={shape} interp={interp} {precision}")
+    N = int(np.prod(shape))
+    assert d["nonconverged"] == 0
+    # diagnostics are the sums of the stored state (update.cu:52-69)
+    dims = 1 if lat == 0 else 3
+    f, rho, g = out
+    assert abs(d["mass"] - rho.sum()) <= 1e-12 * rho.sum() + 1e-9
+    assert abs(d["enrg"] - np.sum(rho * (np.sum(g[:3] ** 2, axis=0) + dims * g[3]))) <= 1e-9 * abs(d["enrg"])
+    if precision == "fp64":
+        assert d["niter_max"] == int(niter.max())
+    assert d["istep"] == 2 and 1 <= d["niter_mean"] <= 100 and N > 0
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_sod_shock_d1q5(orc, pond, precision):
+    out, ref, niter, nc, d = run_pair(orc, pond, 0, (256, 1, 1), 4, precision, tau=0.55, nsteps=4, kind="sod")
+    _compare(out, ref, TOL[precision], "sod")
+
+
+@pytest.mark.parametrize("bc", [(1, 0, 0), (2, 0, 0), (1, 1, 1), (2, 2, 2)])
+@pytest.mark.parametrize("lat,shape,interp", [(0, (64, 1, 1), 4), (1, (6, 5, 4), 4), (2, (4, 4, 3), 6),
+                                              (0, (64, 1, 1), 8), (0, (64, 1, 1), 7)])
+def test_boundaries_match_oracle(orc, pond, lat, shape, interp, bc):
+    if lat == 0:
+        bc = (bc[0], 0, 0)
+    out, ref, niter, nc, d = run_pair(orc, pond, lat, shape, interp, "fp64", bc=bc, kind="smooth", seed=5)
+    _compare(out, ref, TOL["fp64"], f"bc={bc}")
+
+
+def test_iteration_cap_reports_nonconvergence(orc, pond):
+    shape = (32, 1, 1)
+    out, ref, niter, nc, d = run_pair(orc, pond, 0, shape, 4, "fp64", max_iter=1, nsteps=1)
+    _compare(out, ref, TOL["fp64"], "max_iter=1")
+    assert nc == 32 and d["nonconverged"] == 32 and d["niter_max"] == 1
+
+
+def test_matches_reference_fixtures_directly(pond):
+    """The GPU float64 path against the reference kernels' own outputs."""
+    import glob
+    import os
+    here = os.path.dirname(os.path.abspath(__file__))
+    paths = sorted(glob.glob(os.path.join(here, "golden", "*.npz")))
+    assert paths
+    for p in paths:
+        z = np.load(p)
+        lat = int(z["lattice"]); shape = tuple(int(v) for v in z["shape"])
+        with pond.Solver(lattice=lat, shape=shape, precision="fp64", tau=float(z["tau"])) as s:
+            s.set_state(z["rho_in"], z["g_in"], f=z["f_in"])
+            s.step(int(z["nsteps"]))
+            f, rho, g = s.get_state()
+
+        class R:
+            pass
+        ref = R(); ref.f = z["f_out"]; ref.rho = z["rho_out"]; ref.g = z["g_out"]
+        _compare((f, rho, g), ref, 1e-9, os.path.basename(p))
+
+
+def test_init_and_errors(pond):
+    with pond.Solver(lattice="D1Q5", shape=(64, 1, 1)) as s:
+        with pytest.raises(pond.PondError):
+            s.step(1)  # before init
+        s.init("acoustic")
+        d0 = s.diagnostics()
+        s.step(3)
+        d = s.diagnostics()
+        assert d["istep"] == 3 and d["nonconverged"] == 0
+        assert abs(d["mass"] - d0["mass"]) < 1e-5 * d0["mass"]
+    with pond.Solver(lattice="D3Q27", shape=(16, 16, 16)) as s:
+        s.init("tgv", 0.05, 0.1, 1.0, 5.0 / 3.0)
+        s.step(2)
+        assert s.diagnostics()["k"] > 0
