@@ -1,0 +1,349 @@
+#!/usr/bin/env python
+"""Benchmark of the PonD step on B200: D3Q27, 256^3 spherical Riemann problem.
+
+Workload (the MLUPS metric's configuration): unit box at 256^3, inside r < 0.2
+(rho = 1, p = 1), outside (rho = 0.125, p = 0.1), u = 0, lattice time step
+dt/dx = 0.25 (so T_lattice = 0.0625 p/rho), tau = 0.52, cubic Lagrange
+interpolation (the reference's propagate<4>), float32 populations with float64
+moments and convergence test at |delta| < 1e-8 + 1e-6 |value|.  One "step" is
+one PonD time step of the whole box.  The state (2.1 GB per buffer) is far
+larger than L2, so no flush is needed between steps.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Prints one JSON line.  With --gpus N > 1 (under torchrun) every rank advances
+its own independent box (replicas: the step has no exchange on one GPU per
+problem) and the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MLUPS D3Q27 256^3: learned-gauge vs plain PonD at equal L1 error vs FP64"
+LAMBDA = 0.25            # dt/dx of the lattice
+TAU = 0.52
+TOL_ABS, TOL_REL = 1e-7, 1e-6  # float32 floor: 1e-8 sits below the accumulation noise at rho ~ 1
+BYTES_PER_NODE = (27 + 5) * 4 * 2   # f, rho, u, T read once and written once (float32)
+FLOPS_PER_TRANSFORM = 2 * 3 * 27 * 3  # three 1D passes of a 3x3 basis matrix over 27 populations
+NOMINAL_FP32_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 148 SMs x 128 lanes x FMA at the max SM clock
+
+
+def sphere_params():
+    # cx, cy, cz, radius, rho_in, T_in, rho_out, T_out  (T = lambda^2 p/rho)
+    return (0.5, 0.5, 0.5, 0.2, 1.0, LAMBDA ** 2 * 1.0, 0.125, LAMBDA ** 2 * 0.1 / 0.125)
+
+
+def sphere_state(n):
+    """The same initial condition on the host (for the oracle's sample)."""
+    c = (np.arange(n) + 0.5) / n - 0.5
+    z, y, x = np.meshgrid(c, c, c, indexing="ij")
+    inside = (x * x + y * y + z * z < 0.2 ** 2).reshape(-1)
+    p = sphere_params()
+    rho = np.where(inside, p[4], p[6])
+    T = np.where(inside, p[5], p[7])
+    zero = np.zeros_like(rho)
+    return rho, np.stack([zero, zero, zero, T])
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        finally:
+            os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------------ distributed plumbing
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    return rank, local, world, pg
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def allmax(pg, v):
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ------------------------------------------------------------------ CPU baseline (oracle)
+def cpu_baseline(budget_s=15.0):
+    """FP64 oracle (restated reference step) on a bounded sample of the same
+    initial condition, all host threads."""
+    from oracle import oracle as O
+    O.build()
+    n = 12
+    st = O.base_state(1, *sphere_state(n)[:1], *sphere_state(n)[1])
+    t0 = time.perf_counter()
+    O.step(st, 1, (n, n, n), tau=TAU, tol_abs=TOL_ABS, tol_rel=TOL_REL)
+    dt = time.perf_counter() - t0
+    # grow the sample to use about budget_s of CPU time
+    per_node = dt / n ** 3
+    m = int(max(n, min(40, round((budget_s / per_node) ** (1 / 3)))))
+    rho, g = sphere_state(m)
+    st = O.base_state(1, rho, *g)
+    t0 = time.perf_counter()
+    O.step(st, 1, (m, m, m), tau=TAU, tol_abs=TOL_ABS, tol_rel=TOL_REL)
+    dt = time.perf_counter() - t0
+    return {"value": m ** 3 / dt / 1e6, "unit": "MLUPS", "cores": O.max_threads(), "kind": "port",
+            "sample": f"one step of the same sphere problem at {m}^3 on the FP64 oracle ({dt:.1f} s)"}
+
+
+# ------------------------------------------------------------------ reference kernels on the GPU
+def reference_cuda(n=64):
+    """The reference's own PonDstep (FP64 and FP32 builds), kernel time only."""
+    from tests.golden.make_golden import read_state, write_state
+    out = {}
+    rho, g = sphere_state(n)
+    from oracle import oracle as O
+    w = O.tables(1).w
+    f = w[:, None] * rho[None, :]
+    for prec in ("double", "float"):
+        binary = os.path.join(ROOT, "oracle", "_ref", f"ref_pond_D3Q27_{prec}_{n}x{n}x{n}")
+        if not os.path.exists(binary):
+            out[prec] = None
+            continue
+        with tempfile.TemporaryDirectory() as td:
+            fin, fout = os.path.join(td, "in"), os.path.join(td, "out")
+            write_state(fin, f, rho, g, (n, n, n))
+            r = subprocess.run([binary, fin, fout, "2", repr(TAU)], capture_output=True, text=True, timeout=900)
+            if r.returncode != 0:
+                out[prec] = {"error": r.stderr[-300:]}
+                continue
+            _, _, _, nmax, ms = read_state(fout, 27, (n, n, n))
+        out[prec] = {"ms_per_step": float(ms[-1]), "MLUPS": n ** 3 / (float(ms[-1]) / 1e3) / 1e6,
+                     "niter_max": nmax, "grid": f"{n}^3"}
+    return out
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(args, rank, local, world, pg):
+    import torch
+
+    import lbmpond_b200 as pond
+    n = args.size
+    N = n ** 3
+    s = pond.Solver(lattice="D3Q27", shape=(n, n, n), interp=pond.LAGR4, precision="fp32", tau=TAU,
+                    tol_abs=TOL_ABS, tol_rel=TOL_REL, device=local)
+    s.init("sphere", *sphere_params())
+    s.step(args.warmup)
+    s.last_step_ms()
+    barrier(pg)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        s.step(args.steps)
+        ms_total = s.last_step_ms()
+    torch.cuda.synchronize()
+    barrier(pg)
+    d = s.diagnostics()
+    work = s.last_step_work()
+    ms_step = allmax(pg, ms_total / args.steps)
+    value = world * N / (ms_step / 1e3) / 1e6
+    clocks = clk.summary()
+
+    # e2e through the C ABI with host buffers: upload the state from pinned
+    # host memory, step, read back rho/u/T (the reference's drop() fields)
+    e2e = None
+    if not args.no_e2e:
+        f_h = torch.empty((27, N), dtype=torch.float32, pin_memory=True)
+        r_h = torch.empty(N, dtype=torch.float32, pin_memory=True)
+        g_h = torch.empty((4, N), dtype=torch.float32, pin_memory=True)
+        s.download_native(f_h.data_ptr(), r_h.data_ptr(), g_h.data_ptr())  # host snapshot of the state
+        ro_h = torch.empty(N, dtype=torch.float32, pin_memory=True)
+        go_h = torch.empty((4, N), dtype=torch.float32, pin_memory=True)
+        stream = torch.cuda.ExternalStream(s.stream(), device=local)
+        k = max(1, min(args.steps, 5))
+        s.upload_native(f_h.data_ptr(), r_h.data_ptr(), g_h.data_ptr())
+        s.step(1)
+        s.download_native(None, ro_h.data_ptr(), go_h.data_ptr())
+        barrier(pg)
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(k):
+            s.upload_native(f_h.data_ptr(), r_h.data_ptr(), g_h.data_ptr())
+            s.step(1)
+            s.download_native(None, ro_h.data_ptr(), go_h.data_ptr())
+        ev1.record(stream)
+        ev1.synchronize()
+        e2e_ms = allmax(pg, ev0.elapsed_time(ev1) / k)
+        e2e = {"value": world * N / (e2e_ms / 1e3) / 1e6, "unit": "MLUPS",
+               "h2d_bytes_per_step": (27 + 5) * N * 4, "d2h_bytes_per_step": 5 * N * 4, "ms_per_step": e2e_ms}
+
+    achieved_gbs = BYTES_PER_NODE * N / (ms_step / 1e3) / 1e9
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        tj = json.load(open(tpath))
+        t = tj.get("pull_d3q27_lagr4_f32")
+        if t and t.get("bytes_per_node"):
+            traffic = t["bytes_per_node"] * N
+    flops = work * FLOPS_PER_TRANSFORM
+    tflops = flops / (ms_step / 1e3) / 1e12
+    s.close()
+    return {
+        "metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"D3Q27 {n}^3 spherical Riemann problem, tau {TAU}, cubic Lagrange, "
+                               f"tolerance {TOL_ABS:g}+{TOL_REL:g}|v|", "path": "plain",
+                   "grid": [n, n, n], "lattice": "D3Q27", "interp": "lagrange4", "precision": "fp32 (fp64 moments)",
+                   "l2": "inputs larger than L2 (2.15 GB state per buffer)",
+                   "parallelism": "replicas" if world > 1 else "single"},
+        "iterations": {"mean": d["niter_mean"], "max": d["niter_max"], "nonconverged": d["nonconverged"]},
+        "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": achieved_gbs / hbm_peak, "traffic": traffic, "peak_source": "measured",
+                     "algorithmic_bytes_per_node": BYTES_PER_NODE},
+        "roofline_fp32": {"bound": "fp32", "achieved": tflops, "peak": NOMINAL_FP32_TFLOPS, "unit": "TFLOP/s",
+                          "frac": tflops / NOMINAL_FP32_TFLOPS, "peak_source": "nominal at 1965 MHz",
+                          "flops_per_step": flops, "transformed_nodes_per_step": work},
+        "e2e": e2e,
+        "gpu_launches": args.steps,
+        "clocks": clocks,
+    }
+
+
+def run_reference(args, rank, world):
+    """The reference arm: the reference's step restated on the host (FP64
+    oracle; the reference itself has no CPU implementation), all host threads,
+    each step a bounded sample of the same problem."""
+    from oracle import oracle as O
+    O.build()
+    m = args.ref_size
+    rho, g = sphere_state(m)
+    st0 = O.base_state(1, rho, *g)
+    for _ in range(args.warmup):
+        O.step(st0, 1, (m, m, m), tau=TAU, tol_abs=TOL_ABS, tol_rel=TOL_REL)
+    t0 = time.perf_counter()
+    st = st0
+    for _ in range(args.steps):
+        st, niter, _ = O.step(st, 1, (m, m, m), tau=TAU, tol_abs=TOL_ABS, tol_rel=TOL_REL)
+    dt = (time.perf_counter() - t0) / args.steps
+    v = m ** 3 / dt / 1e6
+    sample = f"{m}^3 sample of the sphere problem per step (FP64 oracle, {O.max_threads()} threads)"
+    return {"impl": "reference", "metric": METRIC, "value": v, "unit": "MLUPS", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"D3Q27 spherical Riemann problem (sample {m}^3), tau {TAU}, cubic Lagrange",
+                       "path": "reference step on the host"},
+            "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": O.max_threads(), "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": v, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--ref-size", type=int, default=12)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--ref-cuda", action="store_true", help="also time the reference's own kernels (64^3)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        if rank != 0:
+            return
+        print(json.dumps(run_reference(args, rank, world)), flush=True)
+        return
+    rank, local, world, pg = dist_setup(args.gpus)
+    out = run_ours(args, rank, local, world, pg)
+    if rank == 0 and world == 1 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_baseline()
+    if rank == 0 and args.ref_cuda:
+        out["reference_cuda"] = reference_cuda()
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -138,6 +138,15 @@ void* pond_stream(pond_ctx* ctx);
 int pond_device_state(pond_ctx* ctx, void** f, void** rho, void** g);
 /* synchronous device-time of the last pond_step call's step kernels, in ms */
 int pond_last_step_ms(pond_ctx* ctx, float* ms);
+/* host transfers in the context's own precision (float for POND_FP32, double
+   for POND_FP64), no conversion: f[Q*N], rho[N], g[4*N]; pinned host memory
+   gives full PCIe bandwidth.  pond_upload_state writes the current buffer only. */
+int pond_upload_state(pond_ctx* ctx, const void* f, const void* rho, const void* g);
+/* any of f, rho, g may be NULL */
+int pond_download_state(pond_ctx* ctx, void* f, void* rho, void* g);
+/* stencil nodes transformed during the last step, summed over nodes and
+   iterations (the work count behind the compute roofline) */
+int pond_last_step_work(pond_ctx* ctx, int64_t* transformed_nodes);
 
 #ifdef __cplusplus
 }

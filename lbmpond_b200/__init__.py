@@ -151,6 +151,21 @@ class Solver:
         _lib.check(self._L.pond_last_step_ms(self._ctx, ctypes.byref(ms)))
         return float(ms.value)
 
+    def last_step_work(self) -> int:
+        w = ctypes.c_int64()
+        _lib.check(self._L.pond_last_step_work(self._ctx, ctypes.byref(w)))
+        return int(w.value)
+
+    def upload_native(self, f, rho, g):
+        """Host arrays already in the context's precision (C-contiguous, ideally pinned)."""
+        _lib.check(self._L.pond_upload_state(self._ctx, ctypes.c_void_p(f), ctypes.c_void_p(rho),
+                                             ctypes.c_void_p(g)))
+
+    def download_native(self, f=None, rho=None, g=None):
+        """Copy the state to host arrays in the context's precision (any may be None)."""
+        vp = lambda a: ctypes.c_void_p(a) if a else None  # noqa: E731
+        _lib.check(self._L.pond_download_state(self._ctx, vp(f), vp(rho), vp(g)))
+
     def stream(self) -> int:
         return int(self._L.pond_stream(self._ctx) or 0)
 

@@ -65,6 +65,9 @@ SIGNATURES = {
     "pond_stream": (_vp, [_vp]),
     "pond_device_state": (ctypes.c_int, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
     "pond_last_step_ms": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_float)]),
+    "pond_upload_state": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    "pond_download_state": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    "pond_last_step_work": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int64)]),
 }
 
 _lib = None

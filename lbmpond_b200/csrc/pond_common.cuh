@@ -135,6 +135,7 @@ __device__ __forceinline__ int resolve_axis(int p, int n, int bc, bool* rev) {
 struct StepSums {
   double mass, mom[3], enrg, k;
   unsigned long long niter_sum, nonconv;
+  unsigned long long work;  // stencil nodes transformed (summed over nodes and iterations)
   int niter_max;
   int pad;
 };

@@ -108,7 +108,7 @@ int download(pond_ctx* c, const void* src, size_t count, double* dst) {
 template <typename R>
 __global__ void state_sums_kernel(const R* rho, const R* g, long long N, double dim, double kdx, StepSums* out) {
   const long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  NodeSums ns = {0, 0, 0, 0, 0, 0, 0ull, 0ull, 0};
+  NodeSums ns = {0, 0, 0, 0, 0, 0, 0ull, 0ull, 0ull, 0};
   if (n < N) {
     const double r = rho[n], u0 = g[n], u1 = g[N + n], u2 = g[2 * N + n], T = g[3 * N + n];
     const double u2s = u0 * u0 + u1 * u1 + u2 * u2;

@@ -30,7 +30,7 @@ __global__ void __launch_bounds__(128) pull_1d_scheme_kernel(StepArgs<R> a) {
   constexpr int NS = SCHEME == POND_TVD ? 4 : 5;  // slots per population
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const bool active = x < a.nx;
-  NodeSums ns = {0, 0, 0, 0, 0, 0, 0ull, 0ull, 0};
+  NodeSums ns = {0, 0, 0, 0, 0, 0, 0ull, 0ull, 0ull, 0};
   if (active) {
     const long long idx = x;
     R f0[Q];
@@ -75,6 +75,7 @@ __global__ void __launch_bounds__(128) pull_1d_scheme_kernel(StepArgs<R> a) {
       for (int k = 0; k < Q; k++)
 #pragma unroll
         for (int m = 0; m < NS; m++) acc[k][m] = R(0);
+      ns.work += (unsigned long long)(hi - lo + 1);
       for (int p = lo; p <= hi; p++) {
         bool rv[3] = {false, false, false};
         const int rx = resolve_axis(p, a.nx, a.bc[0], &rv[0]);

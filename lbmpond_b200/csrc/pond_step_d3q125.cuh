@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(D125_THREADS) pull_d3q125_kernel(StepArgs<R> a
     a.f_out[(long long)tid * a.N + idx] = f0;
   }
   const R rs = R(rho0), u0 = R(U[0]), u1 = R(U[1]), u2 = R(U[2]), ts = R(T);
-  NodeSums ns = {0, 0, 0, 0, 0, 0, 0ull, 0ull, 0};
+  NodeSums ns = {0, 0, 0, 0, 0, 0, 0ull, 0ull, 0ull, 0};
   if (tid == 0) {
     a.rho_out[idx] = rs;
     a.g_out[idx] = u0; a.g_out[a.N + idx] = u1; a.g_out[2 * a.N + idx] = u2; a.g_out[3 * a.N + idx] = ts;
@@ -192,6 +192,7 @@ __global__ void __launch_bounds__(D125_THREADS) pull_d3q125_kernel(StepArgs<R> a
     ns.enrg = dr * (u2s + L::Dim * dt);
     ns.k = a.kdx * u2s;
     ns.niter = niter; ns.nonconv = conv ? 0 : 1; ns.nmax = niter;
+    ns.work = 27ull * niter;
   }
   reduce_and_commit(ns, a.sums);
 }

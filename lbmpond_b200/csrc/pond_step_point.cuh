@@ -59,12 +59,12 @@ template <int N, typename R> __device__ __forceinline__ R pick(const R w[N], int
 // context's StepSums (one atomic per block and quantity).
 struct NodeSums {
   double mass, m0, m1, m2, enrg, k;
-  unsigned long long niter, nonconv;
+  unsigned long long niter, nonconv, work;
   int nmax;
 };
 __device__ __forceinline__ void reduce_and_commit(NodeSums s, StepSums* out) {
   __shared__ double sd[6][32];
-  __shared__ unsigned long long su[2][32];
+  __shared__ unsigned long long su[3][32];
   __shared__ int si[32];
   const int lane = threadIdx.x & 31;
   const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
@@ -77,20 +77,21 @@ __device__ __forceinline__ void reduce_and_commit(NodeSums s, StepSums* out) {
     for (int q = 0; q < 6; q++) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
     s.niter += __shfl_xor_sync(0xffffffffu, s.niter, o);
     s.nonconv += __shfl_xor_sync(0xffffffffu, s.nonconv, o);
+    s.work += __shfl_xor_sync(0xffffffffu, s.work, o);
     s.nmax = max(s.nmax, __shfl_xor_sync(0xffffffffu, s.nmax, o));
   }
   if ((tid & 31) == 0) {
     for (int q = 0; q < 6; q++) sd[q][warp] = v[q];
-    su[0][warp] = s.niter; su[1][warp] = s.nonconv; si[warp] = s.nmax;
+    su[0][warp] = s.niter; su[1][warp] = s.nonconv; su[2][warp] = s.work; si[warp] = s.nmax;
   }
   __syncthreads();
   if (tid == 0) {
     double t[6] = {0, 0, 0, 0, 0, 0};
-    unsigned long long a = 0, b = 0;
+    unsigned long long a = 0, b = 0, c = 0;
     int m = 0;
     for (int w = 0; w < nwarps; w++) {
       for (int q = 0; q < 6; q++) t[q] += sd[q][w];
-      a += su[0][w]; b += su[1][w]; m = max(m, si[w]);
+      a += su[0][w]; b += su[1][w]; c += su[2][w]; m = max(m, si[w]);
     }
     atomicAdd(&out->mass, t[0]);
     atomicAdd(&out->mom[0], t[1]);
@@ -100,6 +101,7 @@ __device__ __forceinline__ void reduce_and_commit(NodeSums s, StepSums* out) {
     atomicAdd(&out->k, t[5]);
     atomicAdd(&out->niter_sum, a);
     atomicAdd(&out->nonconv, b);
+    if (c) atomicAdd(&out->work, c);
     atomicMax(&out->niter_max, m);
   }
   (void)lane;
@@ -274,7 +276,7 @@ __global__ void __launch_bounds__(128) pull_point_kernel(StepArgs<R> a) {
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int z = blockIdx.z * blockDim.z + threadIdx.z;
   const bool active = x < a.nx && y < a.ny && z < a.nz;
-  NodeSums ns = {0, 0, 0, 0, 0, 0, 0ull, 0ull, 0};
+  NodeSums ns = {0, 0, 0, 0, 0, 0, 0ull, 0ull, 0ull, 0};
   if (active) {
     const long long idx = x + (long long)a.nx * (y + (long long)a.ny * z);
     R f0[Q];
@@ -323,6 +325,7 @@ __global__ void __launch_bounds__(128) pull_point_kernel(StepArgs<R> a) {
           lo[ax] = hi[ax] = pos[ax];
         }
       }
+      ns.work += (unsigned long long)(hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
       for (int px = lo[0]; px <= hi[0]; px++) {
         bool rv[3] = {false, false, false};
         const int rx = resolve_axis((int)px, dims[0], a.bc[0], &rv[0]);
