@@ -5,7 +5,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include "../../include/pond.h"
+#include "pond.h"
 
 namespace pond {
 
@@ -118,13 +118,13 @@ template <typename R> struct Basis<5, R> {
 
 // Boundary resolution of a stencil coordinate along one axis.  Returns the
 // in-range index and sets *rev when the mirror boundary reflected it.
-__device__ __forceinline__ int resolve_axis(int p, int n, int bc, bool* rev) {
-  *rev = false;
+__device__ __forceinline__ int resolve_axis(int p, int n, int bc, bool& rev) {
+  rev = false;
   if (p >= 0 && p < n) return p;
   if (bc == POND_BC_CLAMP) return p < 0 ? 0 : n - 1;
   if (bc == POND_BC_MIRROR) {
-    if (p < 0) { p = -1 - p; *rev = true; }
-    if (p >= n) { p = n - 1 - p + n; *rev = true; }
+    if (p < 0) { p = -1 - p; rev = true; }
+    if (p >= n) { p = n - 1 - p + n; rev = true; }
   }
   p %= n;
   return p < 0 ? p + n : p;

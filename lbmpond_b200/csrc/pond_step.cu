@@ -2,11 +2,13 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "pond_internal.h"
 #include "pond_step_1d.cuh"
 #include "pond_step_d3q125.cuh"
+#include "pond_step_d3q27.cuh"
 #include "pond_step_point.cuh"
 
 namespace pond {
@@ -193,6 +195,19 @@ template <typename R> static int launch_typed(pond_ctx* c) {
       }
       break;
     case POND_D3Q27:
+      if constexpr (std::is_same<R, float>::value) {
+        if (c->p.interp >= POND_LAGR2 && c->p.interp <= POND_LAGR4) {
+          dim3 blk(d27::TX, d27::TY, d27::TZ);
+          dim3 grd((a.nx + d27::TX - 1) / d27::TX, (a.ny + d27::TY - 1) / d27::TY, (a.nz + d27::TZ - 1) / d27::TZ);
+          void (*kern)(StepArgs<float>) = c->p.interp == POND_LAGR2   ? d27::pull_d3q27_tile_kernel<2>
+                                          : c->p.interp == POND_LAGR3 ? d27::pull_d3q27_tile_kernel<3>
+                                                                      : d27::pull_d3q27_tile_kernel<4>;
+          e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d27::SMEM_BYTES);
+          if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+          kern<<<grd, blk, d27::SMEM_BYTES, s>>>(a);
+          break;
+        }
+      }
       switch (c->p.interp) {
         case POND_LAGR2: launch_point<POND_D3Q27, 2, R>(a, s); break;
         case POND_LAGR3: launch_point<POND_D3Q27, 3, R>(a, s); break;

@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(128) pull_1d_scheme_kernel(StepArgs<R> a) {
       ns.work += (unsigned long long)(hi - lo + 1);
       for (int p = lo; p <= hi; p++) {
         bool rv[3] = {false, false, false};
-        const int rx = resolve_axis(p, a.nx, a.bc[0], &rv[0]);
+        const int rx = resolve_axis(p, a.nx, a.bc[0], rv[0]);
         R fn[Q], s[3], r[3];
         const R Ucs[3] = {Uc, R(0), R(0)};
         load_node<POND_D1Q5, R>(a, rx, rv, Ucs, invC, fn, s, r);

@@ -40,9 +40,9 @@ __global__ void __launch_bounds__(D125_THREADS) pull_d3q125_kernel(StepArgs<R> a
   // ---- stage the 3x3x3 stencil (steps.cu:164-193)
   for (int n = 0; n < 27; n++) {
     bool rv[3];
-    const int px = resolve_axis(x - 1 + n / 9, a.nx, a.bc[0], &rv[0]);
-    const int py = resolve_axis(y - 1 + (n / 3) % 3, a.ny, a.bc[1], &rv[1]);
-    const int pz = resolve_axis(z - 1 + n % 3, a.nz, a.bc[2], &rv[2]);
+    const int px = resolve_axis(x - 1 + n / 9, a.nx, a.bc[0], rv[0]);
+    const int py = resolve_axis(y - 1 + (n / 3) % 3, a.ny, a.bc[1], rv[1]);
+    const int pz = resolve_axis(z - 1 + n % 3, a.nz, a.bc[2], rv[2]);
     const long long nidx = px + (long long)a.nx * (py + (long long)a.ny * pz);
     if (own) S.f[n][tid] = finite_or_zero_f(a.f_in[(long long)tid * a.N + nidx]);
     if (tid < 3) {

@@ -328,19 +328,19 @@ __global__ void __launch_bounds__(128) pull_point_kernel(StepArgs<R> a) {
       ns.work += (unsigned long long)(hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
       for (int px = lo[0]; px <= hi[0]; px++) {
         bool rv[3] = {false, false, false};
-        const int rx = resolve_axis((int)px, dims[0], a.bc[0], &rv[0]);
+        const int rx = resolve_axis((int)px, dims[0], a.bc[0], rv[0]);
         R wx[Q1];
 #pragma unroll
         for (int c = 0; c < Q1; c++) wx[c] = pick<N, R>(wt[0][c], org[0][c], px);
         for (int py = lo[1]; py <= hi[1]; py++) {
-          const int ry = (D == 3) ? resolve_axis((int)py, dims[1], a.bc[1], &rv[1]) : (int)py;
+          const int ry = (D == 3) ? resolve_axis((int)py, dims[1], a.bc[1], rv[1]) : (int)py;
           R wy[Q1];
           if (D == 3) {
 #pragma unroll
             for (int c = 0; c < Q1; c++) wy[c] = pick<N, R>(wt[1][c], org[1][c], py);
           }
           for (int pz = lo[2]; pz <= hi[2]; pz++) {
-            const int rz = (D == 3) ? resolve_axis((int)pz, dims[2], a.bc[2], &rv[2]) : (int)pz;
+            const int rz = (D == 3) ? resolve_axis((int)pz, dims[2], a.bc[2], rv[2]) : (int)pz;
             const long long nidx = rx + (long long)a.nx * (ry + (long long)a.ny * rz);
             R fn[Q], s[3], r[3];
             load_node<LAT, R>(a, nidx, rv, Uc, invC, fn, s, r);

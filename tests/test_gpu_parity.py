@@ -100,14 +100,35 @@ def test_sod_shock_d1q5(orc, pond, precision):
     _compare(out, ref, TOL[precision], "sod")
 
 
-@pytest.mark.parametrize("bc", [(1, 0, 0), (2, 0, 0), (1, 1, 1), (2, 2, 2)])
-@pytest.mark.parametrize("lat,shape,interp", [(0, (64, 1, 1), 4), (1, (6, 5, 4), 4), (2, (4, 4, 3), 6),
-                                              (0, (64, 1, 1), 8), (0, (64, 1, 1), 7)])
-def test_boundaries_match_oracle(orc, pond, lat, shape, interp, bc):
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("bc", [(1, 0, 0), (2, 0, 0), (1, 1, 1), (2, 2, 2), (0, 2, 1)])
+@pytest.mark.parametrize("lat,shape,interp", [(0, (64, 1, 1), 4), (1, (6, 5, 4), 4), (1, (33, 9, 5), 3),
+                                              (2, (4, 4, 3), 6), (0, (64, 1, 1), 8), (0, (64, 1, 1), 7)])
+def test_boundaries_match_oracle(orc, pond, lat, shape, interp, bc, precision):
     if lat == 0:
         bc = (bc[0], 0, 0)
-    out, ref, niter, nc, d = run_pair(orc, pond, lat, shape, interp, "fp64", bc=bc, kind="smooth", seed=5)
-    _compare(out, ref, TOL["fp64"], f"bc={bc}")
+    out, ref, niter, nc, d = run_pair(orc, pond, lat, shape, interp, precision, bc=bc, kind="smooth", seed=5)
+    _compare(out, ref, TOL[precision], f"bc={bc}")
+
+
+@pytest.mark.parametrize("interp", [2, 3, 4])
+def test_d3q27_departures_beyond_staged_halo(orc, pond, interp):
+    """A fast, hot flow (|u| + sqrt(T/TLat) > 1) sends departure points past the
+    float32 kernel's staged +-2 halo; those lanes read global memory."""
+    shape = (40, 6, 4)
+    rho, g = smooth_state(shape, 3, seed=9, modes=1, du=0.05)
+    g[0] += 0.75
+    g[3] = 0.12 * (1 + 0.1 * np.sin(np.arange(rho.size)))
+    f = perturbed_populations(orc, 1, rho, g, seed=9, eps=0.01)
+    st = orc.State(f, rho, g)
+    with pond.Solver(lattice=1, shape=shape, interp=interp, precision="fp32", tau=0.8) as s:
+        s.set_state(rho, g, f=f)
+        s.step(2)
+        out = s.get_state()
+    ref = st
+    for _ in range(2):
+        ref, niter, nc = orc.step(ref, 1, shape, interp=interp, tau=0.8)
+    _compare(out, ref, TOL["fp32"], "fast flow")
 
 
 def test_iteration_cap_reports_nonconvergence(orc, pond):
