@@ -28,13 +28,21 @@ constexpr int TX = 32, TY = 4, TZ = 2, H = 2;
 constexpr int SX = TX + 2 * H, SY = TY + 2 * H, SZ = TZ + 2 * H;
 constexpr int SN = SX * SY * SZ;  // 1728 staged nodes
 constexpr int NPL = 31;           // planes: 27 f, u_x, u_y, u_z, c
-constexpr size_t SMEM_BYTES = size_t(NPL) * SN * sizeof(float) + SN;  // + per-node flags
+// + a global node index (int32) and a flag byte per staged node
+constexpr size_t SMEM_BYTES = size_t(NPL) * SN * sizeof(float) + size_t(SN) * sizeof(int) + SN;
 constexpr int THREADS = TX * TY * TZ;
 
 // reference population index of tensor class t = 9 cx + 3 cy + cz, for
 // lookups with run-time indices (consts.h:20-30 order)
 __constant__ int c_ref27[27] = {0, 3, 16, 2, 6, 18, 12, 13, 24, 1, 5, 17, 4, 7, 19, 14, 15, 25,
                                 8, 10, 22, 9, 11, 23, 20, 21, 26};
+
+// 4-byte asynchronous global -> shared copy and the wait for all of them
+__device__ __forceinline__ void cp_async4(float* dst, const float* src) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // class index -> its mirror image along one axis (0 <-> 0, + <-> -)
 __device__ __forceinline__ int rev3(int c) { return c == 0 ? 0 : 3 - c; }
@@ -86,6 +94,52 @@ __device__ __forceinline__ void transform_accumulate(const float fn[27], const f
       }
 }
 
+// As transform_accumulate, restricted to the target classes each axis needs
+// at this stencil node (nx/ny/nz: warp-uniform, a class is skipped when its
+// interpolation weight is zero for every lane of the warp).
+__device__ __forceinline__ void transform_accumulate_sel(const float fn[27], const float Mx[3][3],
+                                                         const float My[3][3], const float Mz[3][3],
+                                                         const bool nx[3], const bool ny[3], const bool nz[3],
+                                                         float acc[27]) {
+  float t1[3][3][3];
+#pragma unroll
+  for (int iz = 0; iz < 3; iz++) {
+    if (!nz[iz]) continue;
+#pragma unroll
+    for (int jx = 0; jx < 3; jx++)
+#pragma unroll
+      for (int jy = 0; jy < 3; jy++)
+        t1[jx][jy][iz] = fmaf(Mz[iz][2], fn[jx * 9 + jy * 3 + 2],
+                              fmaf(Mz[iz][1], fn[jx * 9 + jy * 3 + 1], Mz[iz][0] * fn[jx * 9 + jy * 3]));
+  }
+  float t2[3][3][3];
+#pragma unroll
+  for (int iy = 0; iy < 3; iy++) {
+    if (!ny[iy]) continue;
+#pragma unroll
+    for (int iz = 0; iz < 3; iz++) {
+      if (!nz[iz]) continue;
+#pragma unroll
+      for (int jx = 0; jx < 3; jx++)
+        t2[jx][iy][iz] = fmaf(My[iy][2], t1[jx][2][iz], fmaf(My[iy][1], t1[jx][1][iz], My[iy][0] * t1[jx][0][iz]));
+    }
+  }
+#pragma unroll
+  for (int ix = 0; ix < 3; ix++) {
+    if (!nx[ix]) continue;
+#pragma unroll
+    for (int iy = 0; iy < 3; iy++) {
+      if (!ny[iy]) continue;
+#pragma unroll
+      for (int iz = 0; iz < 3; iz++) {
+        if (!nz[iz]) continue;
+        float& o = acc[ix * 9 + iy * 3 + iz];
+        o = fmaf(Mx[ix][2], t2[2][iy][iz], fmaf(Mx[ix][1], t2[1][iy][iz], fmaf(Mx[ix][0], t2[0][iy][iz], o)));
+      }
+    }
+  }
+}
+
 // interpolation weight of relative offset o for a window starting at ro
 template <int N> __device__ __forceinline__ float wpick(const float w[N], int ro, int o) {
   const int j = o - ro;
@@ -99,54 +153,66 @@ template <int N>
 __global__ void __launch_bounds__(THREADS, 1) pull_d3q27_tile_kernel(StepArgs<float> a) {
   using L = Lattice<POND_D3Q27>;
   extern __shared__ __align__(16) float sm[];
-  unsigned char* flags = reinterpret_cast<unsigned char*>(sm + NPL * SN);
+  int* gidx = reinterpret_cast<int*>(sm + NPL * SN);
+  unsigned char* flags = reinterpret_cast<unsigned char*>(gidx + SN);
   const int tid = threadIdx.x + TX * (threadIdx.y + TY * threadIdx.z);
   const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z0 = blockIdx.z * TZ;
 
-  // ---- stage the gauge planes (and per-node mirror/validity flags)
+  // ---- stage the tile: every value is fetched with an asynchronous copy
+  // (cp.async, no register round trip), so a thread has all of its ~210
+  // copies in flight at once; boundary resolution happens in the addresses.
+  // 1) per staged node: global index, mirror flags, the four gauge planes
   for (int i = tid; i < SN; i += THREADS) {
     const int hx = i % SX, hy = (i / SX) % SY, hz = i / (SX * SY);
     bool rv[3];
     const int gx = resolve_axis(x0 - H + hx, a.nx, a.bc[0], rv[0]);
     const int gy = resolve_axis(y0 - H + hy, a.ny, a.bc[1], rv[1]);
     const int gz = resolve_axis(z0 - H + hz, a.nz, a.bc[2], rv[2]);
-    const long long g = gx + (long long)a.nx * (gy + (long long)a.ny * gz);
+    const int g = gx + a.nx * (gy + a.ny * gz);
+    gidx[i] = g;
+    flags[i] = (unsigned char)((rv[0] ? 1 : 0) | (rv[1] ? 2 : 0) | (rv[2] ? 4 : 0));
+#pragma unroll
+    for (int k = 0; k < 4; k++) cp_async4(&sm[(27 + k) * SN + i], a.g_in + (long long)k * a.N + g);
+  }
+  __syncthreads();
+  // 2) populations in tensor-class order (the mirror reverses classes)
+  for (int idx = tid; idx < 27 * SN; idx += THREADS) {
+    const int p = idx / SN, i = idx - p * SN;
+    const unsigned fl = flags[i];
+    int cx = p / 9, cy = (p / 3) % 3, cz = p % 3;
+    if (fl & 1) cx = rev3(cx);
+    if (fl & 2) cy = rev3(cy);
+    if (fl & 4) cz = rev3(cz);
+    cp_async4(&sm[idx], a.f_in + (long long)c_ref27[cx * 9 + cy * 3 + cz] * a.N + gidx[i]);
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  // 3) gauge post-pass: mirrored velocity components flip sign, c = sqrts(T/TLat);
+  //    a node with a non-finite gauge contributes nothing (all its transfer
+  //    terms are non-finite in the reference and dropped)
+  for (int i = tid; i < SN; i += THREADS) {
+    const unsigned fl = flags[i];
     float u[3];
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-      const float v = a.g_in[(long long)k * a.N + g];
-      u[k] = rv[k] ? -v : v;
+      const float v = sm[(27 + k) * SN + i];
+      u[k] = (fl >> k) & 1 ? -v : v;
     }
-    const float T = a.g_in[3 * a.N + g];
+    const float T = sm[30 * SN + i];
     const float c = copysignf(sqrtf(fabsf(T) * (float)(1.0 / L::TLat)), T);
     const bool ok = fabsf(u[0]) <= 3.0e38f && fabsf(u[1]) <= 3.0e38f && fabsf(u[2]) <= 3.0e38f && fabsf(c) <= 3.0e38f;
     sm[27 * SN + i] = ok ? u[0] : 0.f;
     sm[28 * SN + i] = ok ? u[1] : 0.f;
     sm[29 * SN + i] = ok ? u[2] : 0.f;
     sm[30 * SN + i] = ok ? c : 1.f;
-    flags[i] = (unsigned char)((ok ? 0 : 8) | (rv[0] ? 1 : 0) | (rv[1] ? 2 : 0) | (rv[2] ? 4 : 0));
+    flags[i] = (unsigned char)(fl | (ok ? 0 : 8));
   }
   __syncthreads();
-  // ---- stage the populations in tensor-class order (mirror reversal, non-finite -> 0)
+  // 4) populations post-pass: non-finite values and invalid nodes -> 0
   for (int idx = tid; idx < 27 * SN; idx += THREADS) {
-    const int p = idx / SN, i = idx - p * SN;
-    const int hx = i % SX, hy = (i / SX) % SY, hz = i / (SX * SY);
-    const unsigned fl = flags[i];
-    float v = 0.f;
-    if (!(fl & 8)) {
-      bool rv[3];
-      const int gx = resolve_axis(x0 - H + hx, a.nx, a.bc[0], rv[0]);
-      const int gy = resolve_axis(y0 - H + hy, a.ny, a.bc[1], rv[1]);
-      const int gz = resolve_axis(z0 - H + hz, a.nz, a.bc[2], rv[2]);
-      int cx = p / 9, cy = (p / 3) % 3, cz = p % 3;
-      if (fl & 1) cx = rev3(cx);
-      if (fl & 2) cy = rev3(cy);
-      if (fl & 4) cz = rev3(cz);
-      const long long g = gx + (long long)a.nx * (gy + (long long)a.ny * gz);
-      v = a.f_in[(long long)c_ref27[cx * 9 + cy * 3 + cz] * a.N + g];
-      v = fabsf(v) <= 3.402823466e38f ? v : 0.f;
-    }
-    sm[idx] = v;
+    const int i = idx % SN;
+    const float v = sm[idx];
+    sm[idx] = (!(flags[i] & 8) && fabsf(v) <= 3.402823466e38f) ? v : 0.f;
   }
   __syncthreads();
 
@@ -204,18 +270,30 @@ __global__ void __launch_bounds__(THREADS, 1) pull_d3q27_tile_kernel(StepArgs<fl
       if (!done) work += (unsigned long long)(wh[0] - wl[0] + 1) * (wh[1] - wl[1] + 1) * (wh[2] - wl[2] + 1);
       for (int ox = wl[0]; ox <= wh[0]; ox++) {
         float wx[3];
+        bool nx[3];
 #pragma unroll
-        for (int c = 0; c < 3; c++) wx[c] = wpick<N>(wt[0][c], ro[0][c], ox);
+        for (int c = 0; c < 3; c++) {
+          wx[c] = wpick<N>(wt[0][c], ro[0][c], ox);
+          nx[c] = __any_sync(0xffffffffu, !done && wx[c] != 0.f);
+        }
         for (int oy = wl[1]; oy <= wh[1]; oy++) {
           float wy[3];
+          bool ny[3];
 #pragma unroll
-          for (int c = 0; c < 3; c++) wy[c] = wpick<N>(wt[1][c], ro[1][c], oy);
+          for (int c = 0; c < 3; c++) {
+            wy[c] = wpick<N>(wt[1][c], ro[1][c], oy);
+            ny[c] = __any_sync(0xffffffffu, !done && wy[c] != 0.f);
+          }
 #pragma unroll
           for (int oz = -H; oz <= H; oz++) {
             if (oz < wl[2] || oz > wh[2]) continue;
             float wz[3];
+            bool nz[3];
 #pragma unroll
-            for (int c = 0; c < 3; c++) wz[c] = wpick<N>(wt[2][c], ro[2][c], oz);
+            for (int c = 0; c < 3; c++) {
+              wz[c] = wpick<N>(wt[2][c], ro[2][c], oz);
+              nz[c] = __any_sync(0xffffffffu, !done && wz[c] != 0.f);
+            }
             const int si = sbase + oz * SX * SY + oy * SX + ox;
             float fn[27];
 #pragma unroll
@@ -226,7 +304,7 @@ __global__ void __launch_bounds__(THREADS, 1) pull_d3q27_tile_kernel(StepArgs<fl
             weighted_rows(fmaf(sm[27 * SN + si], invC, -Us[0]), r, wx, Mx);
             weighted_rows(fmaf(sm[28 * SN + si], invC, -Us[1]), r, wy, My);
             weighted_rows(fmaf(sm[29 * SN + si], invC, -Us[2]), r, wz, Mz);
-            transform_accumulate(fn, Mx, My, Mz, acc);
+            transform_accumulate_sel(fn, Mx, My, Mz, nx, ny, nz, acc);
           }
         }
       }
