@@ -148,6 +148,34 @@ int pond_download_state(pond_ctx* ctx, void* f, void* rho, void* g);
    iterations (the work count behind the compute roofline) */
 int pond_last_step_work(pond_ctx* ctx, int64_t* transformed_nodes);
 
+/* Allocation-free step.  This entry point has no counterpart in the
+   reference, which only steps its own global buffers.
+
+   One D3Q27 float32 step (Lagrange order 2-4, params->interp) from the
+   caller's device buffers f_in/rho_in/g_in into f_out/rho_out/g_out (layout
+   as above, float, N = Nx*Ny*Nz nodes), with the step's diagnostics written
+   to diag_out, a pond_diag in DEVICE memory; istep and curtime are left 0.
+   Work is queued on `stream` (a cudaStream_t, 0 = legacy default stream); the
+   call does not synchronise.  params->device is ignored: the current device
+   is used.
+
+   It is meant for callers that cannot let a library call cudaMalloc: code
+   that owns all device memory through its own pool or a budget fixed at
+   start-up, or that must not stall on an allocation inside its time loop.
+   It calls no cudaMalloc, cudaFree or allocating library routine.  Its only
+   scratch, one partial-sum record per step CTA, lives in a fixed
+   POND_NOALLOC_SCRATCH_BYTES array in the library's device memory, which
+   every GPU that loads the library holds until the process exits.  Grids that
+   need more than 65536 step CTAs (more than 256^3 nodes, counted in 32x4x2
+   tiles) are rejected with POND_ERR_ARG.  The first call on each device looks
+   up that array's device address (and opts the kernel into its shared
+   memory); make that first call before any stream capture.  All calls share
+   the array and every call rewrites it: calls whose kernels overlap on a GPU
+   (other streams, other threads) race on it. */
+#define POND_NOALLOC_SCRATCH_BYTES 5242880
+int pond_step_noalloc(const pond_params* params, const float* f_in, const float* rho_in, const float* g_in,
+                      float* f_out, float* rho_out, float* g_out, pond_diag* diag_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

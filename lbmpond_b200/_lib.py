@@ -68,6 +68,7 @@ SIGNATURES = {
     "pond_upload_state": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "pond_download_state": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "pond_last_step_work": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int64)]),
+    "pond_step_noalloc": (ctypes.c_int, [ctypes.POINTER(PondParams)] + [_vp] * 8),
 }
 
 _lib = None

@@ -149,7 +149,50 @@ template <int N> __device__ __forceinline__ float wpick(const float w[N], int ro
   return r;
 }
 
-template <int N>
+// Per-CTA partial of the step sums, written instead of the atomic update
+// when the kernel runs without a context (kPartials = true; a.sums then
+// points at an array of one BlockPartial per CTA).
+struct BlockPartial {
+  double mass, mom[3], enrg, k;
+  unsigned long long niter_sum, nonconv, work;
+  int niter_max;
+  int pad;
+};
+
+__device__ __forceinline__ void write_block_partial(NodeSums s, BlockPartial* out) {
+  __shared__ double pd[6][THREADS / 32];
+  __shared__ unsigned long long pu[3][THREADS / 32];
+  __shared__ int pm[THREADS / 32];
+  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int warp = tid >> 5;
+  double v[6] = {s.mass, s.m0, s.m1, s.m2, s.enrg, s.k};
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+    for (int q = 0; q < 6; q++) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+    s.niter += __shfl_xor_sync(0xffffffffu, s.niter, o);
+    s.nonconv += __shfl_xor_sync(0xffffffffu, s.nonconv, o);
+    s.work += __shfl_xor_sync(0xffffffffu, s.work, o);
+    s.nmax = max(s.nmax, __shfl_xor_sync(0xffffffffu, s.nmax, o));
+  }
+  if ((tid & 31) == 0) {
+    for (int q = 0; q < 6; q++) pd[q][warp] = v[q];
+    pu[0][warp] = s.niter; pu[1][warp] = s.nonconv; pu[2][warp] = s.work; pm[warp] = s.nmax;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    BlockPartial b = {};
+    for (int w = 0; w < THREADS / 32; w++) {
+      b.mass += pd[0][w]; b.mom[0] += pd[1][w]; b.mom[1] += pd[2][w]; b.mom[2] += pd[3][w];
+      b.enrg += pd[4][w]; b.k += pd[5][w];
+      b.niter_sum += pu[0][w]; b.nonconv += pu[1][w]; b.work += pu[2][w];
+      b.niter_max = max(b.niter_max, pm[w]);
+    }
+    out[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = b;
+  }
+}
+
+template <int N, bool kPartials = false>
 __global__ void __launch_bounds__(THREADS, 1) pull_d3q27_tile_kernel(StepArgs<float> a) {
   using L = Lattice<POND_D3Q27>;
   extern __shared__ __align__(16) float sm[];
@@ -358,7 +401,8 @@ __global__ void __launch_bounds__(THREADS, 1) pull_d3q27_tile_kernel(StepArgs<fl
     finish_node<POND_D3Q27, float>(a, idx, f0, rho0, U, T, niter, conv, ns);
     ns.work = work;
   }
-  reduce_and_commit(ns, a.sums);
+  if constexpr (kPartials) write_block_partial(ns, reinterpret_cast<BlockPartial*>(a.sums));
+  else reduce_and_commit(ns, a.sums);
 }
 
 }  // namespace d27
