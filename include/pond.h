@@ -148,6 +148,53 @@ int pond_download_state(pond_ctx* ctx, void* f, void* rho, void* g);
    iterations (the work count behind the compute roofline) */
 int pond_last_step_work(pond_ctx* ctx, int64_t* transformed_nodes);
 
+/* ---- learned starting gauge ------------------------------------------
+   A small network (35 -> H -> H -> 4, tanh, H = 64 or 128; BF16 tensor-core
+   GEMMs with float32 accumulation, float32 master weights, Adam) predicts
+   each node's converged gauge from the pre-step (rho, u, T) of the node and
+   its six face neighbours.  The prediction only replaces the starting gauge
+   of the unchanged fixed-point iteration, which still runs to the same
+   tolerance.  Features (35): centre c, u/c (3), T/TLat with c = sqrt(T/TLat);
+   per neighbour (-x,+x,-y,+y,-z,+z) rho_n/rho-1, (u_n-u)/c (3), T_n/T-1.
+   Targets (4): (u*-u)/c (3), (T*-T)/T.  Feature/target rows are float32 in
+   device memory, row-major.  No counterpart in the reference (whose
+   iteration starts from the previous gauge, steps.cu:360). */
+typedef struct pond_mlp pond_mlp;
+int pond_mlp_create(int hidden, uint64_t seed, int device, pond_mlp** out);
+int pond_mlp_destroy(pond_mlp* net);
+int pond_mlp_num_params(const pond_mlp* net);
+/* params: W1[H][35], b1[H], W2[H][H], b2[H], W3[4][H], b3[4];
+   stats: xmean[35], xstd[35], ymean[4], ystd[4] (either pointer may be NULL) */
+int pond_mlp_get_params(pond_mlp* net, float* params, float* stats);
+int pond_mlp_set_params(pond_mlp* net, const float* params, const float* stats);
+/* standardisation statistics from n device rows X[n][35], Y[n][4] */
+int pond_mlp_fit_stats(pond_mlp* net, const float* X, const float* Y, int64_t n);
+/* `steps` Adam steps (beta 0.9/0.999) of mean-squared error on standardised
+   targets, minibatches of `batch` rows taken cyclically; loss_out (host,
+   `steps` floats) may be NULL */
+int pond_mlp_train(pond_mlp* net, const float* X, const float* Y, int64_t n, int batch, int steps, float lr,
+                   float* loss_out);
+/* full-batch gradient (host, num_params floats) and loss; n must be a
+   multiple of the training tile (128 rows for H = 64, 64 for H = 128) */
+int pond_mlp_gradients(pond_mlp* net, const float* X, const float* Y, int64_t n, float* grad, float* loss);
+/* de-standardised outputs Y[n][4] for raw feature rows X[n][35] (device) */
+int pond_mlp_forward(pond_mlp* net, const float* X, float* Y, int64_t n);
+/* training pairs from the last step: pre-step features and the increment to
+   the converged gauge, for nodes offset + k*stride (offset = seed % stride)
+   whose 7-node stencil is not exactly uniform; *written rows (<= capacity),
+   in no particular order; node (device int64[capacity], may be NULL)
+   receives each row's node index */
+int pond_collect_pairs(pond_ctx* ctx, float* X, float* Y, int64_t* node, int64_t capacity, int64_t stride,
+                       uint64_t seed, int64_t* written);
+/* bind a network to a context (NULL detaches): every following pond_step
+   first predicts each node's starting gauge.  A node keeps its previous
+   gauge when its 7-node stencil is exactly uniform or when the largest
+   predicted |change| is below `gate` (in the target units above). */
+int pond_set_predictor(pond_ctx* ctx, pond_mlp* net, float gate);
+/* the starting gauge the bound network predicts for the current state
+   (device float[4*N], planes u_x, u_y, u_z, T) */
+int pond_predict(pond_ctx* ctx, float* guess);
+
 /* Allocation-free step.  This entry point has no counterpart in the
    reference, which only steps its own global buffers.
 

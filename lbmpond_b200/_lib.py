@@ -69,6 +69,19 @@ SIGNATURES = {
     "pond_download_state": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "pond_last_step_work": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int64)]),
     "pond_step_noalloc": (ctypes.c_int, [ctypes.POINTER(PondParams)] + [_vp] * 8),
+    "pond_mlp_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(_vp)]),
+    "pond_mlp_destroy": (ctypes.c_int, [_vp]),
+    "pond_mlp_num_params": (ctypes.c_int, [_vp]),
+    "pond_mlp_get_params": (ctypes.c_int, [_vp, _vp, _vp]),
+    "pond_mlp_set_params": (ctypes.c_int, [_vp, _vp, _vp]),
+    "pond_mlp_fit_stats": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int64]),
+    "pond_mlp_train": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_float, _vp]),
+    "pond_mlp_gradients": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int64, _vp, _vp]),
+    "pond_mlp_forward": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int64]),
+    "pond_collect_pairs": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int64, ctypes.c_int64, ctypes.c_uint64,
+                                          ctypes.POINTER(ctypes.c_int64)]),
+    "pond_set_predictor": (ctypes.c_int, [_vp, _vp, ctypes.c_float]),
+    "pond_predict": (ctypes.c_int, [_vp, _vp]),
 }
 
 _lib = None

@@ -24,6 +24,7 @@ struct pond_ctx {
   float* guess = nullptr;  // [4][N] predicted starting gauge (learned path)
   bool guess_ready = false;
   void* predictor = nullptr;  // learned-gauge network bound to this context
+  float gate = 0.f;           // minimum predicted change that replaces the previous gauge
   bool initialized = false;
   long long istep = 0;
   double curtime = 0;

@@ -1,0 +1,114 @@
+"""Learned starting gauge for the PonD iteration (host-side front end).
+
+`Predictor` wraps a pond_mlp (35 -> H -> H -> 4, BF16 tensor-core kernels,
+float32 master weights, Adam; all arithmetic in libpond_b200.so).  Training
+pairs come from plain steps (`collect_pairs`); device buffers for them are
+torch tensors (plumbing only).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+NIN, NOUT = 35, 4
+
+
+class Predictor:
+    def __init__(self, hidden=64, seed=0, device=0):
+        L = _lib.load()
+        h = ctypes.c_void_p()
+        _lib.check(L.pond_mlp_create(int(hidden), int(seed), int(device), ctypes.byref(h)))
+        self._L, self._h = L, h
+        self.hidden = hidden
+        self.device = device
+        self.nparams = L.pond_mlp_num_params(h)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.pond_mlp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- parameters
+    def get_params(self):
+        p = np.empty(self.nparams, np.float32)
+        st = np.empty(2 * NIN + 2 * NOUT, np.float32)
+        _lib.check(self._L.pond_mlp_get_params(self._h, p.ctypes.data, st.ctypes.data))
+        return p, st
+
+    def set_params(self, params=None, stats=None):
+        p = None if params is None else np.ascontiguousarray(params, np.float32)
+        s = None if stats is None else np.ascontiguousarray(stats, np.float32)
+        _lib.check(self._L.pond_mlp_set_params(self._h, p.ctypes.data if p is not None else None,
+                                               s.ctypes.data if s is not None else None))
+
+    def save(self, path):
+        p, st = self.get_params()
+        np.savez(path, params=p, stats=st, hidden=self.hidden)
+
+    @classmethod
+    def load(cls, path, device=0):
+        z = np.load(path)
+        pr = cls(int(z["hidden"]), device=device)
+        pr.set_params(z["params"], z["stats"])
+        return pr
+
+    # -- training (X, Y: torch float32 CUDA tensors [n, 35], [n, 4])
+    def fit_stats(self, X, Y):
+        _lib.check(self._L.pond_mlp_fit_stats(self._h, X.data_ptr(), Y.data_ptr(), X.shape[0]))
+
+    def train(self, X, Y, steps=1000, batch=4096, lr=2e-3):
+        loss = np.empty(steps, np.float32)
+        _lib.check(self._L.pond_mlp_train(self._h, X.data_ptr(), Y.data_ptr(), X.shape[0], int(batch), int(steps),
+                                          float(lr), loss.ctypes.data))
+        return loss
+
+    def gradients(self, X, Y):
+        g = np.empty(self.nparams, np.float32)
+        loss = np.empty(1, np.float32)
+        _lib.check(self._L.pond_mlp_gradients(self._h, X.data_ptr(), Y.data_ptr(), X.shape[0], g.ctypes.data,
+                                              loss.ctypes.data))
+        return float(loss[0]), g
+
+    def forward(self, X, out=None):
+        import torch
+        if out is None:
+            out = torch.empty((X.shape[0], NOUT), dtype=torch.float32, device=X.device)
+        _lib.check(self._L.pond_mlp_forward(self._h, X.data_ptr(), out.data_ptr(), X.shape[0]))
+        return out
+
+
+def collect_pairs(solver, X, Y, offset_rows=0, stride=7, seed=0, nodes=None):
+    """Append the pairs of the solver's last step to rows [offset_rows, ...)
+    of the torch buffers X [cap, 35] and Y [cap, 4] (and their node indices
+    to the int64 buffer `nodes`, if given); returns rows written."""
+    L = _lib.load()
+    cap = X.shape[0] - offset_rows
+    if cap <= 0:
+        return 0
+    n = ctypes.c_int64()
+    xp = X.data_ptr() + offset_rows * NIN * 4
+    yp = Y.data_ptr() + offset_rows * NOUT * 4
+    np_ = nodes.data_ptr() + offset_rows * 8 if nodes is not None else None
+    _lib.check(L.pond_collect_pairs(solver.handle, xp, yp, np_, int(cap), int(stride), int(seed), ctypes.byref(n)))
+    return int(n.value)
+
+
+def attach(solver, predictor, gate=0.0):
+    """Start every following step of `solver` from the predicted gauge
+    (None detaches)."""
+    L = _lib.load()
+    _lib.check(L.pond_set_predictor(solver.handle, predictor.handle if predictor else None, float(gate)))
+    solver.params.learned = 1 if predictor else 0
