@@ -195,42 +195,133 @@ def reference_cuda(n=64):
 
 
 # ------------------------------------------------------------------ our arm
+def _timed_window(s, pg, steps, warmup):
+    """W untimed warm-up steps, then K steps timed with CUDA events on the
+    library's stream, bracketed by a barrier and a synchronisation."""
+    import torch
+    s.step(warmup)
+    s.last_step_ms()
+    barrier(pg)
+    torch.cuda.synchronize()
+    d0 = s.diagnostics()
+    s.step(steps)
+    ms = s.last_step_ms()
+    torch.cuda.synchronize()
+    barrier(pg)
+    d1 = s.diagnostics()
+    return ms / steps, d0, d1
+
+
+def _l1(a, b):
+    return float(np.abs(a - b).mean() / np.abs(b).mean())
+
+
 def run_ours(args, rank, local, world, pg):
     import torch
 
     import lbmpond_b200 as pond
+    from lbmpond_b200.learned import Predictor, attach, calibrate_gate, collect_pairs, keep_history
     n = args.size
     N = n ** 3
-    s = pond.Solver(lattice="D3Q27", shape=(n, n, n), interp=pond.LAGR4, precision="fp32", tau=TAU,
-                    tol_abs=TOL_ABS, tol_rel=TOL_REL, device=local)
+    mk = lambda prec="fp32": pond.Solver(lattice="D3Q27", shape=(n, n, n), interp=pond.LAGR4,  # noqa: E731
+                                        precision=prec, tau=TAU,
+                                        tol_abs=TOL_ABS if prec == "fp32" else None,
+                                        tol_rel=TOL_REL if prec == "fp32" else None, device=local)
+    s = mk()
     s.init("sphere", *sphere_params())
-    t_spin = time.perf_counter()
-    s.step(args.spinup)
-    s.last_step_ms()
-    t_spin = time.perf_counter() - t_spin
-    s.step(args.warmup)
-    s.last_step_ms()
-    barrier(pg)
+    # spin-up (untimed), collecting training pairs over its last steps
+    cap = args.pair_capacity
+    X = torch.empty((cap, 39), dtype=torch.float32, device="cuda")
+    Y = torch.empty((cap, 4), dtype=torch.float32, device="cuda")
+    rows = 0
+    t0 = time.perf_counter()
+    for k in range(args.spinup):
+        collect = args.learned and k >= args.spinup - args.collect_steps and rows < cap
+        if collect:
+            keep_history(s, True)
+        s.step(1)
+        if collect:
+            rows += collect_pairs(s, X, Y, offset_rows=rows, stride=args.pair_stride, seed=k)
+    keep_history(s, False)
     torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
-        s.step(args.steps)
-        ms_total = s.last_step_ms()
-    torch.cuda.synchronize()
-    barrier(pg)
-    d = s.diagnostics()
-    work = s.last_step_work()
-    ms_step = allmax(pg, ms_total / args.steps)
-    value = world * N / (ms_step / 1e3) / 1e6
-    clocks = clk.summary()
+    t_spin = time.perf_counter() - t0
+    snap = mk()
+    snap.copy_state_from(s)
 
-    # e2e through the C ABI with host buffers: upload the state from pinned
-    # host memory, step, read back rho/u/T (the reference's drop() fields)
+    # plain path
+    ms_plain, p0, p1 = _timed_window(s, pg, args.steps, args.warmup)
+    ms_plain = allmax(pg, ms_plain)
+    work = s.last_step_work()
+    plain = {"value": world * N / (ms_plain / 1e3) / 1e6, "ms_per_step": ms_plain,
+             "iterations_mean": p1["niter_mean"], "iterations_max": p1["niter_max"],
+             "nonconverged": p1["nonconverged"]}
+
+    # learned path from the same state
+    learned = None
+    net = None
+    if args.learned:
+        t0 = time.perf_counter()
+        net = Predictor(64, seed=0, device=local)
+        net.fit_stats(X[:rows], Y[:rows])
+        loss = net.train(X[:rows], Y[:rows], steps=args.train_steps, batch=8192, lr=2e-3)
+        gate, _ = calibrate_gate(net, X[:rows], Y[:rows])
+        torch.cuda.synchronize()
+        t_train = time.perf_counter() - t0
+        s.copy_state_from(snap)
+        attach(s, net, gate=gate)
+        with ClockSampler(local) as clk:
+            ms_learned, l0, l1d = _timed_window(s, pg, args.steps, args.warmup)
+        ms_learned = allmax(pg, ms_learned)
+        work = s.last_step_work()
+        learned = {"value": world * N / (ms_learned / 1e3) / 1e6, "ms_per_step": ms_learned,
+                   "iterations_mean": l1d["niter_mean"], "iterations_max": l1d["niter_max"],
+                   "nonconverged": l1d["nonconverged"],
+                   "training": {"pairs": rows, "adam_steps": args.train_steps, "batch": 8192,
+                                "loss_first": float(loss[:10].mean()), "loss_last": float(loss[-50:].mean()),
+                                "seconds": t_train, "network": "39-64-64-4 tanh, bf16 tensor cores, fp32 accumulate",
+                                "start": "previous gauge + predicted increment on nodes whose last increment >= gate",
+                                "gate": gate}}
+        d_first, d_last = l0, l1d
+    else:
+        with ClockSampler(local) as clk:
+            pass
+        d_first, d_last = p0, p1
+    clocks = clk.summary()
+    path = "learned" if learned else "plain"
+    head = learned if learned else plain
+    ms_step = head["ms_per_step"]
+    value = head["value"]
+
+    # equal L1 error: a few steps from the snapshot on the float64 path (the
+    # reference-precision result) against the float32 plain and learned paths
+    l1 = None
+    if not args.no_l1 and world == 1:
+        ref64 = mk("fp64")
+        ref64.copy_state_from(snap)
+        ref64.step(args.l1_steps)
+        fr = ref64.fields()
+        ref64.close()
+        l1 = {"steps": args.l1_steps, "reference": "float64 GPU path (tolerance 1e-12 + 1e-10|v|)"}
+        for name, use in (("plain", None), ("learned", net)):
+            if name == "learned" and net is None:
+                continue
+            t = mk()
+            t.copy_state_from(snap)
+            if use is not None:
+                attach(t, use, gate=learned["training"]["gate"])
+            t.step(args.l1_steps)
+            ft = t.fields()
+            t.close()
+            l1[name] = {"rho": _l1(ft["rho"], fr["rho"]), "T": _l1(ft["T"], fr["T"])}
+
+    # e2e through the C ABI with host buffers on the timed path: upload the
+    # state from pinned host memory, step, read back rho/u/T (drop() fields)
     e2e = None
     if not args.no_e2e:
         f_h = torch.empty((27, N), dtype=torch.float32, pin_memory=True)
         r_h = torch.empty(N, dtype=torch.float32, pin_memory=True)
         g_h = torch.empty((4, N), dtype=torch.float32, pin_memory=True)
-        s.download_native(f_h.data_ptr(), r_h.data_ptr(), g_h.data_ptr())  # host snapshot of the state
+        s.download_native(f_h.data_ptr(), r_h.data_ptr(), g_h.data_ptr())
         ro_h = torch.empty(N, dtype=torch.float32, pin_memory=True)
         go_h = torch.empty((4, N), dtype=torch.float32, pin_memory=True)
         stream = torch.cuda.ExternalStream(s.stream(), device=local)
@@ -249,7 +340,7 @@ def run_ours(args, rank, local, world, pg):
         ev1.record(stream)
         ev1.synchronize()
         e2e_ms = allmax(pg, ev0.elapsed_time(ev1) / k)
-        e2e = {"value": world * N / (e2e_ms / 1e3) / 1e6, "unit": "MLUPS",
+        e2e = {"value": world * N / (e2e_ms / 1e3) / 1e6, "unit": "MLUPS", "path": path,
                "h2d_bytes_per_step": (27 + 5) * N * 4, "d2h_bytes_per_step": 5 * N * 4, "ms_per_step": e2e_ms}
 
     achieved_gbs = BYTES_PER_NODE * N / (ms_step / 1e3) / 1e9
@@ -262,25 +353,31 @@ def run_ours(args, rank, local, world, pg):
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
-        tj = json.load(open(tpath))
-        t = tj.get("pull_d3q27_lagr4_f32")
+        t = json.load(open(tpath)).get("pull_d3q27_lagr4_f32")
         if t and t.get("bytes_per_node"):
             traffic = t["bytes_per_node"] * N
-    flops = work * FLOPS_PER_TRANSFORM
+    flops = work * FLOPS_PER_TRANSFORM  # work of the last timed step
     tflops = flops / (ms_step / 1e3) / 1e12
-    s.close()
-    return {
+    drift = {"mass_per_step": (d_last["mass"] - d_first["mass"]) / d_first["mass"] / args.steps,
+             "energy_per_step": (d_last["enrg"] - d_first["enrg"]) / d_first["enrg"] / args.steps}
+    for obj in (s, snap):
+        obj.close()
+    if net is not None:
+        net.close()
+    out = {
         "metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"D3Q27 {n}^3 spherical Riemann problem, tau {TAU}, cubic Lagrange, "
-                               f"tolerance {TOL_ABS:g}+{TOL_REL:g}|v|", "path": "plain",
+                               f"tolerance {TOL_ABS:g}+{TOL_REL:g}|v|", "path": path,
                    "grid": [n, n, n], "lattice": "D3Q27", "interp": "lagrange4", "precision": "fp32 (fp64 moments)",
                    "l2": "inputs larger than L2 (2.15 GB state per buffer)",
                    "parallelism": "replicas" if world > 1 else "single",
-                   "spinup_steps": args.spinup, "timed_steps": f"{args.spinup + args.warmup + 1}.."
-                                                                 f"{args.spinup + args.warmup + args.steps}"},
-        "iterations": {"mean": d["niter_mean"], "max": d["niter_max"], "nonconverged": d["nonconverged"]},
+                   "spinup_steps": args.spinup, "spinup_seconds": t_spin,
+                   "timed_steps": f"{args.spinup + args.warmup + 1}..{args.spinup + args.warmup + args.steps}"},
+        "plain": plain, "learned": learned,
+        "speedup_learned_vs_plain": (learned["value"] / plain["value"]) if learned else None,
+        "l1_vs_fp64": l1, "drift": drift,
         "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved_gbs / hbm_peak, "traffic": traffic, "peak_source": "measured",
                      "algorithmic_bytes_per_node": BYTES_PER_NODE},
@@ -288,9 +385,10 @@ def run_ours(args, rank, local, world, pg):
                           "frac": tflops / NOMINAL_FP32_TFLOPS, "peak_source": "nominal at 1965 MHz",
                           "flops_per_step": flops, "transformed_nodes_per_step": work},
         "e2e": e2e,
-        "gpu_launches": args.steps,
+        "gpu_launches": args.steps * (2 if learned else 1),
         "clocks": clocks,
     }
+    return out
 
 
 def run_reference(args, rank, world):
@@ -329,6 +427,13 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--size", type=int, default=256)
     ap.add_argument("--spinup", type=int, default=150, help="untimed steps before the warm-up")
+    ap.add_argument("--no-learned", dest="learned", action="store_false")
+    ap.add_argument("--collect-steps", type=int, default=30, help="spin-up steps that feed training pairs")
+    ap.add_argument("--pair-stride", type=int, default=61)
+    ap.add_argument("--pair-capacity", type=int, default=4_000_000)
+    ap.add_argument("--train-steps", type=int, default=3000)
+    ap.add_argument("--no-l1", action="store_true")
+    ap.add_argument("--l1-steps", type=int, default=3)
     ap.add_argument("--ref-size", type=int, default=12)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")

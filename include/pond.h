@@ -130,6 +130,8 @@ int pond_diagnostics(pond_ctx* ctx, pond_diag* out);
 /* per-node iteration counts of the last step (int32[N]); needs pond_keep_niter(ctx, 1) before the step */
 int pond_keep_niter(pond_ctx* ctx, int on);
 int pond_get_niter(pond_ctx* ctx, int32_t* niter);
+/* keep the gauge of one more time level (needed by pond_collect_pairs) */
+int pond_keep_history(pond_ctx* ctx, int on);
 
 /* the context's CUDA stream (a cudaStream_t) */
 void* pond_stream(pond_ctx* ctx);
@@ -144,30 +146,36 @@ int pond_last_step_ms(pond_ctx* ctx, float* ms);
 int pond_upload_state(pond_ctx* ctx, const void* f, const void* rho, const void* g);
 /* any of f, rho, g may be NULL */
 int pond_download_state(pond_ctx* ctx, void* f, void* rho, void* g);
+/* copy the state of src into dst (same lattice and grid; the precision is
+   converted on the device): both stored time levels and the step counter */
+int pond_copy_state(pond_ctx* dst, pond_ctx* src);
 /* stencil nodes transformed during the last step, summed over nodes and
    iterations (the work count behind the compute roofline) */
 int pond_last_step_work(pond_ctx* ctx, int64_t* transformed_nodes);
 
 /* ---- learned starting gauge ------------------------------------------
-   A small network (35 -> H -> H -> 4, tanh, H = 64 or 128; BF16 tensor-core
+   A small network (39 -> H -> H -> 4, tanh, H = 64 or 128; BF16 tensor-core
    GEMMs with float32 accumulation, float32 master weights, Adam) predicts
    each node's converged gauge from the pre-step (rho, u, T) of the node and
-   its six face neighbours.  The prediction only replaces the starting gauge
-   of the unchanged fixed-point iteration, which still runs to the same
-   tolerance.  Features (35): centre c, u/c (3), T/TLat with c = sqrt(T/TLat);
-   per neighbour (-x,+x,-y,+y,-z,+z) rho_n/rho-1, (u_n-u)/c (3), T_n/T-1.
-   Targets (4): (u*-u)/c (3), (T*-T)/T.  Feature/target rows are float32 in
-   device memory, row-major.  No counterpart in the reference (whose
-   iteration starts from the previous gauge, steps.cu:360). */
+   its six face neighbours and the node's last gauge increment.  The
+   prediction only replaces the starting gauge of the unchanged fixed-point
+   iteration, which still runs to the same tolerance.
+   Features (39), c = sqrt(T/TLat): centre c, u/c (3), T/TLat; per neighbour
+   (-x,+x,-y,+y,-z,+z) rho_m/rho-1, (u_m-u)/c (3), T_m/T-1; the centre's last
+   increment (u^n-u^{n-1})/c (3), (T^n-T^{n-1})/T.
+   Targets (4): the step's increment of the gauge, (u*-u)/c (3), (T*-T)/T.
+   Feature/target rows are float32 in device memory, row-major.  No
+   counterpart in the reference (whose iteration starts from the previous
+   gauge, steps.cu:360). */
 typedef struct pond_mlp pond_mlp;
 int pond_mlp_create(int hidden, uint64_t seed, int device, pond_mlp** out);
 int pond_mlp_destroy(pond_mlp* net);
 int pond_mlp_num_params(const pond_mlp* net);
-/* params: W1[H][35], b1[H], W2[H][H], b2[H], W3[4][H], b3[4];
-   stats: xmean[35], xstd[35], ymean[4], ystd[4] (either pointer may be NULL) */
+/* params: W1[H][39], b1[H], W2[H][H], b2[H], W3[4][H], b3[4];
+   stats: xmean[39], xstd[39], ymean[4], ystd[4] (either pointer may be NULL) */
 int pond_mlp_get_params(pond_mlp* net, float* params, float* stats);
 int pond_mlp_set_params(pond_mlp* net, const float* params, const float* stats);
-/* standardisation statistics from n device rows X[n][35], Y[n][4] */
+/* standardisation statistics from n device rows X[n][39], Y[n][4] */
 int pond_mlp_fit_stats(pond_mlp* net, const float* X, const float* Y, int64_t n);
 /* `steps` Adam steps (beta 0.9/0.999) of mean-squared error on standardised
    targets, minibatches of `batch` rows taken cyclically; loss_out (host,
@@ -177,20 +185,26 @@ int pond_mlp_train(pond_mlp* net, const float* X, const float* Y, int64_t n, int
 /* full-batch gradient (host, num_params floats) and loss; n must be a
    multiple of the training tile (128 rows for H = 64, 64 for H = 128) */
 int pond_mlp_gradients(pond_mlp* net, const float* X, const float* Y, int64_t n, float* grad, float* loss);
-/* de-standardised outputs Y[n][4] for raw feature rows X[n][35] (device) */
+/* de-standardised outputs Y[n][4] for raw feature rows X[n][39] (device) */
 int pond_mlp_forward(pond_mlp* net, const float* X, float* Y, int64_t n);
-/* training pairs from the last step: pre-step features and the increment to
-   the converged gauge, for nodes offset + k*stride (offset = seed % stride)
-   whose 7-node stencil is not exactly uniform; *written rows (<= capacity),
+/* training pairs from the last step (needs pond_keep_history(ctx, 1) before
+   it): pre-step features and the increment target, for nodes offset +
+   k*stride (offset = seed % stride) whose 7-node stencil is not exactly
+   uniform in space; *written rows (<= capacity),
    in no particular order; node (device int64[capacity], may be NULL)
    receives each row's node index */
 int pond_collect_pairs(pond_ctx* ctx, float* X, float* Y, int64_t* node, int64_t capacity, int64_t stride,
                        uint64_t seed, int64_t* written);
 /* bind a network to a context (NULL detaches): every following pond_step
-   first predicts each node's starting gauge.  A node keeps its previous
-   gauge when its 7-node stencil is exactly uniform or when the largest
-   predicted |change| is below `gate` (in the target units above). */
+   first predicts each node's starting gauge: the previous gauge plus the
+   network's increment on active nodes, i.e. nodes whose 7-node stencil is
+   not exactly uniform and whose last increment (largest of the 4 temporal
+   features) is at least `gate`; other nodes start from the previous gauge. */
 int pond_set_predictor(pond_ctx* ctx, pond_mlp* net, float gate);
+/* without a bound network: start each node from the linear extrapolation
+   g^n + (g^n - g^{n-1}) of its last two gauges (on = 1) or from g^n (on = 0,
+   the reference) */
+int pond_set_extrapolation(pond_ctx* ctx, int on);
 /* the starting gauge the bound network predicts for the current state
    (device float[4*N], planes u_x, u_y, u_z, T) */
 int pond_predict(pond_ctx* ctx, float* guess);

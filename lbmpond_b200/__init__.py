@@ -166,6 +166,10 @@ class Solver:
         vp = lambda a: ctypes.c_void_p(a) if a else None  # noqa: E731
         _lib.check(self._L.pond_download_state(self._ctx, vp(f), vp(rho), vp(g)))
 
+    def copy_state_from(self, other: "Solver"):
+        """Device-side copy of another context's current state (precision converted)."""
+        _lib.check(self._L.pond_copy_state(self._ctx, other._ctx))
+
     def stream(self) -> int:
         return int(self._L.pond_stream(self._ctx) or 0)
 

@@ -62,12 +62,14 @@ SIGNATURES = {
     "pond_diagnostics": (ctypes.c_int, [_vp, ctypes.POINTER(PondDiag)]),
     "pond_keep_niter": (ctypes.c_int, [_vp, ctypes.c_int]),
     "pond_get_niter": (ctypes.c_int, [_vp, _i32p]),
+    "pond_keep_history": (ctypes.c_int, [_vp, ctypes.c_int]),
     "pond_stream": (_vp, [_vp]),
     "pond_device_state": (ctypes.c_int, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
     "pond_last_step_ms": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_float)]),
     "pond_upload_state": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "pond_download_state": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "pond_last_step_work": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int64)]),
+    "pond_copy_state": (ctypes.c_int, [_vp, _vp]),
     "pond_step_noalloc": (ctypes.c_int, [ctypes.POINTER(PondParams)] + [_vp] * 8),
     "pond_mlp_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(_vp)]),
     "pond_mlp_destroy": (ctypes.c_int, [_vp]),
@@ -82,6 +84,7 @@ SIGNATURES = {
                                           ctypes.POINTER(ctypes.c_int64)]),
     "pond_set_predictor": (ctypes.c_int, [_vp, _vp, ctypes.c_float]),
     "pond_predict": (ctypes.c_int, [_vp, _vp]),
+    "pond_set_extrapolation": (ctypes.c_int, [_vp, ctypes.c_int]),
 }
 
 _lib = None

@@ -364,6 +364,20 @@ int pond_keep_niter(pond_ctx* c, int on) {
   return POND_OK;
 }
 
+int pond_keep_history(pond_ctx* c, int on) {
+  if (!c) return set_error(POND_ERR_ARG, "null context");
+  cudaSetDevice(c->p.device);
+  if (on && !c->g_hist) {
+    if (cudaMalloc(&c->g_hist, 4 * (size_t)c->N * c->elem) != cudaSuccess) {
+      cudaGetLastError();
+      c->g_hist = nullptr;
+      return set_error(POND_ERR_NOMEM, "history buffer");
+    }
+  }
+  c->keep_history = on != 0;
+  return POND_OK;
+}
+
 int pond_get_niter(pond_ctx* c, int32_t* out) {
   if (!c || !out) return set_error(POND_ERR_ARG, "null argument");
   if (!c->niter) return set_error(POND_ERR_STATE, "call pond_keep_niter(ctx, 1) before the step");
@@ -433,6 +447,53 @@ int pond_download_state(pond_ctx* c, void* f, void* rho, void* g) {
   if (e == cudaSuccess && g) e = cudaMemcpyAsync(g, c->g[c->cur], 4 * N * c->elem, cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_fail(e, "pond_download_state");
+  return POND_OK;
+}
+
+}  // extern "C"
+
+namespace pond {
+template <typename S, typename D> __global__ void convert_kernel(const S* src, D* dst, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    dst[i] = D(src[i]);
+}
+}  // namespace pond
+
+extern "C" {
+
+int pond_copy_state(pond_ctx* dst, pond_ctx* src) {
+  if (!dst || !src) return set_error(POND_ERR_ARG, "null context");
+  if (dst->p.lattice != src->p.lattice || dst->N != src->N || dst->p.Nx != src->p.Nx || dst->p.Ny != src->p.Ny)
+    return set_error(POND_ERR_ARG, "pond_copy_state: lattice or grid differ");
+  if (dst->p.device != src->p.device) return set_error(POND_ERR_ARG, "pond_copy_state: contexts on different devices");
+  if (!src->initialized) return set_error(POND_ERR_STATE, "source state not initialised");
+  cudaSetDevice(dst->p.device);
+  cudaError_t e = cudaStreamSynchronize(src->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "pond_copy_state");
+  const long long cnt[3] = {(long long)dst->Q * dst->N, dst->N, 4 * dst->N};
+  for (int b = 0; b < 2; b++) {  // both time levels: the current one and the one before it
+    const int sb = b == 0 ? src->cur : 1 - src->cur, db = b == 0 ? dst->cur : 1 - dst->cur;
+    void* d[3] = {dst->f[db], dst->rho[db], dst->g[db]};
+    const void* s3[3] = {src->f[sb], src->rho[sb], src->g[sb]};
+    for (int k = 0; k < 3; k++) {
+      if (dst->elem == src->elem) {
+        e = cudaMemcpyAsync(d[k], s3[k], cnt[k] * dst->elem, cudaMemcpyDeviceToDevice, dst->stream);
+      } else if (dst->elem == 8) {
+        convert_kernel<float, double><<<1024, 256, 0, dst->stream>>>((const float*)s3[k], (double*)d[k], cnt[k]);
+        e = cudaGetLastError();
+      } else {
+        convert_kernel<double, float><<<1024, 256, 0, dst->stream>>>((const double*)s3[k], (float*)d[k], cnt[k]);
+        e = cudaGetLastError();
+      }
+      if (e != cudaSuccess) return cuda_fail(e, "pond_copy_state");
+    }
+  }
+  e = cudaStreamSynchronize(dst->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "pond_copy_state");
+  dst->initialized = true;
+  dst->have_sums = false;
+  dst->istep = src->istep;
+  dst->curtime = src->curtime;
   return POND_OK;
 }
 

@@ -25,6 +25,9 @@ struct pond_ctx {
   bool guess_ready = false;
   void* predictor = nullptr;  // learned-gauge network bound to this context
   float gate = 0.f;           // minimum predicted change that replaces the previous gauge
+  bool extrapolate = false;   // start from g^n + (g^n - g^{n-1}) when no network is bound
+  void* g_hist = nullptr;     // gauge of the level before the last step's input (training pairs)
+  bool keep_history = false;
   bool initialized = false;
   long long istep = 0;
   double curtime = 0;

@@ -285,7 +285,8 @@ __global__ void __launch_bounds__(128) forward_rows_kernel(const float* P, const
 // is below `gate`, keeps its previous gauge.
 template <int H, typename R>
 __global__ void __launch_bounds__(128) predict_kernel(const float* P, const float* stats, const R* rho, const R* g,
-                                                      long long N, int nx, int ny, int nz, int bc0, int bc1,
+                                                      const R* g_old, long long N, int nx, int ny, int nz, int bc0,
+                                                      int bc1,
                                                       int bc2, int lattice, float gate, float* guess) {
   extern __shared__ __align__(16) unsigned char raw[];
   WeightsSmem<H>& W = *reinterpret_cast<WeightsSmem<H>*>(raw);
@@ -298,46 +299,67 @@ __global__ void __launch_bounds__(128) predict_kernel(const float* P, const floa
   const double tlat = lattice == POND_D3Q27 ? 1.0 / 3.0 : 1.0;
   for (long long base = (long long)blockIdx.x * 128; base < N; base += (long long)gridDim.x * 128) {
     const long long n = base + tid;
-    float feat[NIN];
-    bool use = false;
-    if (n < N) use = node_features<R>(rho, g, N, nx, ny, nz, bc, lattice, n, feat);
-#pragma unroll
-    for (int k = 0; k < K1; k++)
-      X[tid][k] = __float2bfloat16((n < N && k < NIN) ? (feat[k] - W.xmean[k]) * W.xistd[k] : 0.f);
-    __syncwarp();
-#pragma unroll
-    for (int mt = 0; mt < 2; mt++) {
-      float h1[H / 8][4], h2[H / 8][4], y[4];
-      forward_tile<H>(W, &X[0][0], K1 + PAD, warp * 32 + mt * 16, lane, h1, h2, y);
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-        const int row = warp * 32 + mt * 16 + gg + 8 * (q >> 1), col = 2 * t + (q & 1);
-        if (col < NOUT) Y[row][col] = y[q];
-      }
-    }
-    __syncwarp();
+    // activity: the largest relative last increment (features 35-38)
+    float act = 0.f, c = 0.f;
+    float cur[4] = {0.f, 0.f, 0.f, 0.f}, old[4] = {0.f, 0.f, 0.f, 0.f};
     if (n < N) {
-      const float ux = g[n], uy = g[N + n], uz = g[2 * N + n], T = g[3 * N + n];
-      float out[4] = {ux, uy, uz, T};
-      if (use) {
-        float d[NOUT];
-        float mx = 0.f;
-        for (int o = 0; o < NOUT; o++) {
-          d[o] = Y[tid][o] * W.ystd[o] + W.ymean[o];
-          mx = fmaxf(mx, fabsf(d[o]));
-        }
-        const float c = sqrtf(fmaxf(T, 0.f) * float(1.0 / tlat));
-        const float Tn = T * (1.f + d[3]);
-        if (mx >= gate && Tn > 0.f && isfinite(Tn)) {
-          out[0] = ux + c * d[0];
-          out[1] = lattice == POND_D1Q5 ? uy : uy + c * d[1];
-          out[2] = lattice == POND_D1Q5 ? uz : uz + c * d[2];
-          out[3] = Tn;
+      for (int k = 0; k < 4; k++) { cur[k] = g[k * N + n]; old[k] = g_old[k * N + n]; }
+      c = sqrtf(fmaxf(cur[3], 0.f) * float(1.0 / tlat));
+      const float ic = c > 0.f ? 1.f / c : 0.f;
+      act = fmaxf(fmaxf(fabsf((cur[0] - old[0]) * ic), fabsf((cur[1] - old[1]) * ic)),
+                  fmaxf(fabsf((cur[2] - old[2]) * ic), cur[3] != 0.f ? fabsf((cur[3] - old[3]) / cur[3]) : 0.f));
+    }
+    const bool active = n < N && act >= gate;
+    float d[NOUT] = {0.f, 0.f, 0.f, 0.f};
+    // a warp gathers features and runs the network only if one of its nodes is active
+    if (__any_sync(0xffffffffu, active)) {
+      float feat[NIN];
+      bool use = false;
+      if (n < N) use = node_features<R>(rho, g, g_old, N, nx, ny, nz, bc, lattice, n, feat);
+#pragma unroll
+      for (int k = 0; k < K1; k++)
+        X[tid][k] = __float2bfloat16((n < N && k < NIN) ? (feat[k] - W.xmean[k]) * W.xistd[k] : 0.f);
+      __syncwarp();
+#pragma unroll
+      for (int mt = 0; mt < 2; mt++) {
+        float h1[H / 8][4], h2[H / 8][4], y[4];
+        forward_tile<H>(W, &X[0][0], K1 + PAD, warp * 32 + mt * 16, lane, h1, h2, y);
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const int row = warp * 32 + mt * 16 + gg + 8 * (q >> 1), col = 2 * t + (q & 1);
+          if (col < NOUT) Y[row][col] = y[q];
         }
       }
+      __syncwarp();
+      if (active && use)
+        for (int o = 0; o < NOUT; o++) d[o] = Y[tid][o] * W.ystd[o] + W.ymean[o];
+    }
+    if (n < N) {
+      // the previous gauge, plus the predicted increment on active nodes
+      float out[4];
+      out[0] = cur[0] + c * d[0];
+      out[1] = lattice == POND_D1Q5 ? cur[1] : cur[1] + c * d[1];
+      out[2] = lattice == POND_D1Q5 ? cur[2] : cur[2] + c * d[2];
+      const float Tn = cur[3] + cur[3] * d[3];
+      out[3] = (Tn > 0.f && isfinite(Tn)) ? Tn : cur[3];
       for (int k = 0; k < 4; k++) guess[k * N + n] = out[k];
     }
     __syncwarp();
+  }
+}
+
+// Starting gauge by linear extrapolation in time from the two stored levels:
+// g* = g^n + (g^n - g^{n-1}); T keeps g^n where the extrapolation is not positive.
+template <typename R>
+__global__ void extrapolate_kernel(const R* g_cur, const R* g_old, long long N, float* guess) {
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < N; n += (long long)gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const float a = g_cur[k * N + n], b = g_old[k * N + n];
+      float v = a + (a - b);
+      if (k == 3 && !(v > 0.f && isfinite(v))) v = a;
+      guess[k * N + n] = v;
+    }
   }
 }
 
@@ -346,7 +368,8 @@ __global__ void __launch_bounds__(128) predict_kernel(const float* P, const floa
 // are sampled with a stride from a random offset; exactly uniform stencils
 // (increment zero by construction) are skipped.
 template <typename R>
-__global__ void pairs_kernel(const R* rho_p, const R* g_p, const R* g_c, long long N, int nx, int ny, int nz,
+__global__ void pairs_kernel(const R* rho_p, const R* g_p, const R* g_h, const R* g_c, long long N, int nx, int ny,
+                             int nz,
                              int bc0, int bc1, int bc2, int lattice, long long offset, long long stride,
                              long long capacity, float* X, float* Y, long long* node_out,
                              unsigned long long* count) {
@@ -355,7 +378,7 @@ __global__ void pairs_kernel(const R* rho_p, const R* g_p, const R* g_c, long lo
   if (n >= N) return;
   const int bc[3] = {bc0, bc1, bc2};
   float feat[NIN];
-  if (!node_features<R>(rho_p, g_p, N, nx, ny, nz, bc, lattice, n, feat)) return;
+  if (!node_features<R>(rho_p, g_p, g_h, N, nx, ny, nz, bc, lattice, n, feat)) return;
   const unsigned long long slot = atomicAdd(count, 1ull);
   if ((long long)slot >= capacity) return;
   for (int i = 0; i < NIN; i++) X[slot * NIN + i] = feat[i];
@@ -364,10 +387,10 @@ __global__ void pairs_kernel(const R* rho_p, const R* g_p, const R* g_c, long lo
   const double T = g_p[3 * N + n];
   const double c = sqrt(fmax(T, 0.0) / tlat);
   const double ic = c > 0 ? 1.0 / c : 0.0;
-  Y[slot * NOUT + 0] = float((double(g_c[n]) - double(g_p[n])) * ic);
-  Y[slot * NOUT + 1] = float((double(g_c[N + n]) - double(g_p[N + n])) * ic);
-  Y[slot * NOUT + 2] = float((double(g_c[2 * N + n]) - double(g_p[2 * N + n])) * ic);
-  Y[slot * NOUT + 3] = float(T != 0 ? (double(g_c[3 * N + n]) - T) / T : 0.0);
+  for (int k = 0; k < 4; k++) {
+    const double r = double(g_c[k * N + n]) - double(g_p[k * N + n]);  // the step's increment
+    Y[slot * NOUT + k] = float(k < 3 ? r * ic : (T != 0 ? r / T : 0.0));
+  }
 }
 
 // Feature/target statistics (float64 sums) for the standardisation.
@@ -439,13 +462,24 @@ static int launch_train(pond_mlp* m, const float* X, const float* Y, long long n
 
 int run_predictor(pond_ctx* c) {
   pond_mlp* m = (pond_mlp*)c->predictor;
-  if (!m) return set_error(POND_ERR_STATE, "learned step without a predictor (pond_set_predictor)");
+  if (!m && !c->extrapolate) return set_error(POND_ERR_STATE, "learned step without a predictor (pond_set_predictor)");
   if (!c->guess) {
     if (cudaMalloc(&c->guess, 4 * sizeof(float) * c->N) != cudaSuccess) {
       cudaGetLastError();
       c->guess = nullptr;
       return set_error(POND_ERR_NOMEM, "predicted gauge buffer");
     }
+  }
+  if (!m) {
+    const int cu = c->cur, od = 1 - c->cur;
+    if (c->elem == 8)
+      mlp::extrapolate_kernel<double><<<1184, 256, 0, c->stream>>>((const double*)c->g[cu], (const double*)c->g[od],
+                                                                   c->N, c->guess);
+    else
+      mlp::extrapolate_kernel<float><<<1184, 256, 0, c->stream>>>((const float*)c->g[cu], (const float*)c->g[od],
+                                                                  c->N, c->guess);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? POND_OK : cuda_fail(e, "extrapolation launch");
   }
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->p.device);
@@ -459,7 +493,8 @@ int run_predictor(pond_ctx* c) {
   e = cudaFuncSetAttribute(mlp::predict_kernel<HH, RR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);   \
   if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");                                               \
   mlp::predict_kernel<HH, RR><<<grid, 128, smem, c->stream>>>(m->P, m->stats, (const RR*)c->rho[cu],               \
-                                                              (const RR*)c->g[cu], c->N, (int)c->p.Nx,             \
+                                                              (const RR*)c->g[cu], (const RR*)c->g[1 - cu], c->N,   \
+                                                              (int)c->p.Nx,                                        \
                                                               (int)c->p.Ny, (int)c->p.Nz, c->p.bc[0], c->p.bc[1], \
                                                               c->p.bc[2], c->p.lattice, gate, c->guess)
   if (m->H == 64) {
@@ -665,6 +700,8 @@ int pond_collect_pairs(pond_ctx* c, float* X, float* Y, int64_t* node, int64_t c
   if (!c || !X || !Y || capacity <= 0 || stride <= 0 || !written)
     return set_error(POND_ERR_ARG, "pond_collect_pairs: bad argument");
   if (c->istep < 1) return set_error(POND_ERR_STATE, "pond_collect_pairs needs a completed step");
+  if (!c->g_hist || !c->keep_history)
+    return set_error(POND_ERR_STATE, "pond_collect_pairs needs pond_keep_history(ctx, 1) before the step");
   cudaSetDevice(c->p.device);
   unsigned long long* d_count = nullptr;
   cudaError_t e = cudaMalloc(&d_count, sizeof(unsigned long long));
@@ -677,12 +714,14 @@ int pond_collect_pairs(pond_ctx* c, float* X, float* Y, int64_t* node, int64_t c
   const int prev = 1 - c->cur, cur = c->cur;
   if (c->elem == 8)
     mlp::pairs_kernel<double><<<blocks, th, 0, c->stream>>>(
-        (const double*)c->rho[prev], (const double*)c->g[prev], (const double*)c->g[cur], c->N, (int)c->p.Nx,
+        (const double*)c->rho[prev], (const double*)c->g[prev], (const double*)c->g_hist, (const double*)c->g[cur],
+        c->N, (int)c->p.Nx,
         (int)c->p.Ny, (int)c->p.Nz, c->p.bc[0], c->p.bc[1], c->p.bc[2], c->p.lattice, offset, stride, capacity, X, Y,
         (long long*)node, d_count);
   else
     mlp::pairs_kernel<float><<<blocks, th, 0, c->stream>>>(
-        (const float*)c->rho[prev], (const float*)c->g[prev], (const float*)c->g[cur], c->N, (int)c->p.Nx,
+        (const float*)c->rho[prev], (const float*)c->g[prev], (const float*)c->g_hist, (const float*)c->g[cur],
+        c->N, (int)c->p.Nx,
         (int)c->p.Ny, (int)c->p.Nz, c->p.bc[0], c->p.bc[1], c->p.bc[2], c->p.lattice, offset, stride, capacity, X, Y,
         (long long*)node, d_count);
   unsigned long long cnt = 0;
@@ -699,8 +738,16 @@ int pond_set_predictor(pond_ctx* c, pond_mlp* m, float gate) {
   if (m && m->device != c->p.device) return set_error(POND_ERR_ARG, "network and context on different devices");
   c->predictor = m;
   c->gate = gate;
-  c->guess_ready = m != nullptr;
-  c->p.learned = m ? 1 : 0;
+  c->guess_ready = m != nullptr || c->extrapolate;
+  c->p.learned = c->guess_ready ? 1 : 0;
+  return POND_OK;
+}
+
+int pond_set_extrapolation(pond_ctx* c, int on) {
+  if (!c) return set_error(POND_ERR_ARG, "null context");
+  c->extrapolate = on != 0;
+  c->guess_ready = c->predictor != nullptr || c->extrapolate;
+  c->p.learned = c->guess_ready ? 1 : 0;
   return POND_OK;
 }
 

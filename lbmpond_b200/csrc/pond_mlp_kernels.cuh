@@ -1,13 +1,15 @@
 // Learned gauge predictor: BF16 tensor-core MLP kernels (mma.sync m16n8k16,
 // float32 accumulation).
 //
-// Network: n_in (35) -> H -> H -> n_out (4), tanh hidden activations.
-// Features of a node (the same function for training pairs and inference):
-//   centre  : c, u_x/c, u_y/c, u_z/c, T/TLat           with c = sqrt(T/TLat)
-//   neighbour (-x,+x,-y,+y,-z,+z): rho_n/rho - 1, (u_n - u)/c (3), T_n/T - 1
-// Targets: (u* - u)/c (3) and (T* - T)/T, u*, T* the converged gauge of the
-// step.  Inputs and targets are standardised with statistics kept in the
-// network.
+// Network: NIN (39) -> H -> H -> NOUT (4), tanh hidden activations.
+// Features of a node at time level n (the same function for training pairs
+// and inference), c = sqrt(T/TLat):
+//   centre  : c, u_x/c, u_y/c, u_z/c, T/TLat
+//   neighbour (-x,+x,-y,+y,-z,+z): rho_m/rho - 1, (u_m - u)/c (3), T_m/T - 1
+//   last increment of the centre: (u^n - u^{n-1})/c (3), (T^n - T^{n-1})/T
+// Target: the step's increment (u* - u^n)/c (3), (T* - T^n)/T, with u*, T*
+// the converged gauge of the step.  Inputs and targets are standardised with
+// statistics kept in the network.
 #pragma once
 #include <cuda_bf16.h>
 
@@ -16,19 +18,22 @@
 namespace pond {
 namespace mlp {
 
-constexpr int NIN = 35;     // 7 nodes x (rho, u_x, u_y, u_z, T)
+constexpr int NIN = 39;     // 7 nodes x (rho, u_x, u_y, u_z, T) + the centre's last increment (4)
 constexpr int NOUT = 4;     // du_x, du_y, du_z, dT
 constexpr int K1 = 48;      // NIN padded to a multiple of 16
 constexpr int OUTP = 16;    // NOUT padded to one m16 tile (8 used as n-tile)
 constexpr int PAD = 8;      // bf16 row padding against shared-memory bank conflicts
 
 // ------------------------------------------------------------------ features
-// Reads the gauge/density planes of the state (any precision) and writes the
-// raw 35 features of node n.  Returns false when the 7-node stencil is
-// exactly uniform (all neighbour differences zero).
+// Reads the gauge/density planes of level n (rho, g) and the gauge of level
+// n-1 (g_old) and writes the raw features of node n.  Returns false when the
+// node's 7-node stencil is exactly uniform in space: there the plain start
+// (the previous gauge) already converges in one iteration, while a uniform
+// far field still carries float32 noise of ~1e-8 from step to step, so a
+// test on the time increment would not separate it.
 template <typename R>
-__device__ __forceinline__ bool node_features(const R* rho, const R* g, long long N, int nx, int ny, int nz,
-                                              const int bc[3], int lattice, long long n, float feat[NIN]) {
+__device__ __forceinline__ bool node_features(const R* rho, const R* g, const R* g_old, long long N, int nx, int ny,
+                                              int nz, const int bc[3], int lattice, long long n, float feat[NIN]) {
   const int x = n % nx, y = (n / nx) % ny, z = n / ((long long)nx * ny);
   const double tlat = lattice == POND_D3Q27 ? 1.0 / 3.0 : 1.0;
   const float rc = rho[n];
@@ -56,6 +61,9 @@ __device__ __forceinline__ bool node_features(const R* rho, const R* g, long lon
     feat[5 + 5 * k + 3] = d3; feat[5 + 5 * k + 4] = d4;
     uniform = uniform && rn == rc && un[0] == ux && un[1] == uy && un[2] == uz && Tn == T;
   }
+  const float ox = g_old[n], oy = g_old[N + n], oz = g_old[2 * N + n], oT = g_old[3 * N + n];
+  feat[35] = (ux - ox) * ic; feat[36] = (uy - oy) * ic; feat[37] = (uz - oz) * ic;
+  feat[38] = T != 0.f ? (T - oT) / T : 0.f;
   return !uniform;
 }
 

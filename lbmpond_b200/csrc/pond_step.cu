@@ -44,6 +44,7 @@ void ctx_free(pond_ctx* c) {
   cudaFree(c->d_sums); c->d_sums = nullptr;
   cudaFree(c->niter); c->niter = nullptr;
   cudaFree(c->guess); c->guess = nullptr;
+  cudaFree(c->g_hist); c->g_hist = nullptr;
   if (c->h_sums) cudaFreeHost(c->h_sums);
   c->h_sums = nullptr;
   if (c->staging) cudaFreeHost(c->staging);
@@ -231,6 +232,11 @@ template <typename R> static int launch_typed(pond_ctx* c) {
 }
 
 int launch_step(pond_ctx* c) {
+  if (c->keep_history && c->g_hist) {  // g^{n-1}, before this step overwrites it
+    cudaError_t e = cudaMemcpyAsync(c->g_hist, c->g[1 - c->cur], 4 * (size_t)c->N * c->elem,
+                                    cudaMemcpyDeviceToDevice, c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "history copy");
+  }
   if (c->p.learned) {
     int st = run_predictor(c);
     if (st != POND_OK) return st;

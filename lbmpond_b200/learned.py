@@ -1,6 +1,6 @@
 """Learned starting gauge for the PonD iteration (host-side front end).
 
-`Predictor` wraps a pond_mlp (35 -> H -> H -> 4, BF16 tensor-core kernels,
+`Predictor` wraps a pond_mlp (39 -> H -> H -> 4, BF16 tensor-core kernels,
 float32 master weights, Adam; all arithmetic in libpond_b200.so).  Training
 pairs come from plain steps (`collect_pairs`); device buffers for them are
 torch tensors (plumbing only).
@@ -13,7 +13,7 @@ import numpy as np
 
 from . import _lib
 
-NIN, NOUT = 35, 4
+NIN, NOUT = 39, 4
 
 
 class Predictor:
@@ -92,7 +92,7 @@ class Predictor:
 
 def collect_pairs(solver, X, Y, offset_rows=0, stride=7, seed=0, nodes=None):
     """Append the pairs of the solver's last step to rows [offset_rows, ...)
-    of the torch buffers X [cap, 35] and Y [cap, 4] (and their node indices
+    of the torch buffers X [cap, 39] and Y [cap, 4] (and their node indices
     to the int64 buffer `nodes`, if given); returns rows written."""
     L = _lib.load()
     cap = X.shape[0] - offset_rows
@@ -104,6 +104,32 @@ def collect_pairs(solver, X, Y, offset_rows=0, stride=7, seed=0, nodes=None):
     np_ = nodes.data_ptr() + offset_rows * 8 if nodes is not None else None
     _lib.check(L.pond_collect_pairs(solver.handle, xp, yp, np_, int(cap), int(stride), int(seed), ctypes.byref(n)))
     return int(n.value)
+
+
+def calibrate_gate(net, X, Y, tol=1e-6, candidates=(0.0, 1e-6, 3e-6, 1e-5, 3e-5, 1e-4, 3e-4, 1e-3, 3e-3, 1e-2,
+                                                  float("inf"))):
+    """Choose the activity gate: the last-increment threshold above which the
+    network's increment replaces the previous gauge as the start.  The score
+    of a candidate is the mean of log10(max |start error| + tol) over the
+    pairs -- the starting error enters the iteration count through its
+    logarithm; below the gate the start error is the increment itself."""
+    import torch
+    pred = net.forward(X)
+    act = X[:, 35:39].abs().max(dim=1).values
+    base = torch.log10(Y.abs().max(dim=1).values + tol)
+    corr = torch.log10((Y - pred).abs().max(dim=1).values + tol)
+    best, best_score = None, None
+    for gt in candidates:
+        use = act >= gt
+        score = float(torch.where(use, corr, base).mean())
+        if best_score is None or score < best_score:
+            best, best_score = gt, score
+    return best, best_score
+
+
+def keep_history(solver, on=True):
+    """Keep one more gauge level so that collect_pairs can run after a step."""
+    _lib.check(_lib.load().pond_keep_history(solver.handle, 1 if on else 0))
 
 
 def attach(solver, predictor, gate=0.0):

@@ -1,21 +1,21 @@
 """Float64 CPU oracle of the learned gauge predictor (TEST INFRASTRUCTURE ONLY).
 
 Restates, in numpy, what the CUDA library's predictor kernels compute: the
-35 node features, the standardisation, the 35 -> H -> H -> 4 tanh network,
+39 node features, the standardisation, the 39 -> H -> H -> 4 tanh network,
 its mean-squared-error loss on standardised targets and the analytic
 gradient.  The GPU kernels run the GEMMs in BF16 with float32 accumulation;
 the tests compare them with this float64 version within BF16 tolerances, and
 check this version against finite differences.
 
 Parameter vector layout (float32 on the device):
-    W1[H][35], b1[H], W2[H][H], b2[H], W3[4][H], b3[4]
-Statistics: xmean[35], xstd[35], ymean[4], ystd[4].
+    W1[H][39], b1[H], W2[H][H], b2[H], W3[4][H], b3[4]
+Statistics: xmean[39], xstd[39], ymean[4], ystd[4].
 """
 from __future__ import annotations
 
 import numpy as np
 
-NIN, NOUT = 35, 4
+NIN, NOUT = 39, 4
 
 
 def unpack(params, H):
@@ -67,9 +67,10 @@ def loss_and_grad(params, H, Xs, Ys):
     return loss, pack(gW1, gb1, gW2, gb2, gW3, gb3)
 
 
-def features(rho, g, shape, lattice=1, bc=(0, 0, 0)):
-    """The 35 features of every node (periodic/clamp/mirror neighbours) and
-    the mask of nodes whose 7-node stencil is not exactly uniform."""
+def features(rho, g, shape, lattice=1, bc=(0, 0, 0), g_old=None):
+    """The 39 features of every node (periodic/clamp/mirror neighbours; the
+    last 4 are the centre's increment from g_old to g) and the mask of nodes
+    whose 7-node stencil is not exactly uniform in space."""
     nx, ny, nz = shape
     N = nx * ny * nz
     tlat = 1.0 / 3.0 if lattice == 1 else 1.0
@@ -108,17 +109,23 @@ def features(rho, g, shape, lattice=1, bc=(0, 0, 0)):
             F[:, 6 + 5 * k + j] = ((Gn[j] - G[j]) * ic).ravel()
         F[:, 9 + 5 * k] = np.where(G[3] != 0, Gn[3] / np.where(G[3] != 0, G[3], 1) - 1, 0).ravel()
         nonuni |= (rn != rho) | (Gn[0] != G[0]) | (Gn[1] != G[1]) | (Gn[2] != G[2]) | (Gn[3] != G[3])
+    Go = G if g_old is None else np.asarray(g_old, np.float64).reshape(4, nz, ny, nx)
+    for k in range(3):
+        F[:, 35 + k] = ((G[k] - Go[k]) * ic).ravel()
+    F[:, 38] = np.where(G[3] != 0, (G[3] - Go[3]) / np.where(G[3] != 0, G[3], 1), 0).ravel()
     return F, nonuni.ravel()
 
 
 def targets(g_prev, g_next, lattice=1):
+    """The step's gauge increment, (u* - u)/c and (T* - T)/T."""
     tlat = 1.0 / 3.0 if lattice == 1 else 1.0
     gp = np.asarray(g_prev, np.float64)
     gn = np.asarray(g_next, np.float64)
     c = np.sqrt(np.maximum(gp[3], 0) / tlat)
     ic = np.where(c > 0, 1 / np.where(c > 0, c, 1), 0)
     Y = np.zeros((gp.shape[1], NOUT))
+    r = gn - gp
     for k in range(3):
-        Y[:, k] = (gn[k] - gp[k]) * ic
-    Y[:, 3] = np.where(gp[3] != 0, (gn[3] - gp[3]) / np.where(gp[3] != 0, gp[3], 1), 0)
+        Y[:, k] = r[k] * ic
+    Y[:, 3] = np.where(gp[3] != 0, r[3] / np.where(gp[3] != 0, gp[3], 1), 0)
     return Y

@@ -86,7 +86,7 @@ def test_training_reduces_loss():
 
 def test_pairs_match_oracle_features(orc, pond):
     torch = _torch()
-    from lbmpond_b200.learned import collect_pairs
+    from lbmpond_b200.learned import collect_pairs, keep_history
     from tests.states import perturbed_populations, smooth_state
     shape = (16, 12, 10)
     N = int(np.prod(shape))
@@ -94,13 +94,14 @@ def test_pairs_match_oracle_features(orc, pond):
     f = perturbed_populations(orc, 1, rho, g, seed=31, eps=0.01)
     with pond.Solver(lattice="D3Q27", shape=shape, precision="fp64", tau=0.8) as s:
         s.set_state(rho, g, f=f)
+        keep_history(s)
         s.step(1)
         _, _, g_next = s.get_state()
         X = torch.zeros((N, M.NIN), dtype=torch.float32, device="cuda")
         Y = torch.zeros((N, M.NOUT), dtype=torch.float32, device="cuda")
         nodes = torch.zeros(N, dtype=torch.int64, device="cuda")
         n = collect_pairs(s, X, Y, stride=1, seed=0, nodes=nodes)
-    F, nonuni = M.features(rho, g, shape)
+    F, nonuni = M.features(rho, g, shape, g_old=g)
     T = M.targets(g, g_next)
     assert n == int(nonuni.sum())
     idx = nodes[:n].cpu().numpy()
@@ -116,7 +117,7 @@ def test_learned_step_keeps_fixed_point_and_cuts_iterations(pond):
     from the same state: the converged states agree to the iteration
     tolerance, and the predicted start needs fewer iterations."""
     torch = _torch()
-    from lbmpond_b200.learned import Predictor, attach, collect_pairs
+    from lbmpond_b200.learned import Predictor, attach, collect_pairs, keep_history
     n = 32
     lam = 0.25
     sphere = (0.5, 0.5, 0.5, 0.2, 1.0, lam * lam, 0.125, lam * lam * 0.8)
@@ -124,12 +125,12 @@ def test_learned_step_keeps_fixed_point_and_cuts_iterations(pond):
     X = torch.zeros((cap, M.NIN), dtype=torch.float32, device="cuda")
     Y = torch.zeros((cap, M.NOUT), dtype=torch.float32, device="cuda")
     rows = 0
-    with pond.Solver(lattice="D3Q27", shape=(n, n, n), precision="fp64", tau=0.52) as s:
-        s.init("sphere", *sphere)
-        for k in range(24):
-            s.step(1)
-            rows += collect_pairs(s, X, Y, offset_rows=rows, stride=1, seed=k)
-        f, rho, g = s.get_state()
+    src = pond.Solver(lattice="D3Q27", shape=(n, n, n), precision="fp64", tau=0.52)
+    src.init("sphere", *sphere)
+    keep_history(src)
+    for k in range(24):
+        src.step(1)
+        rows += collect_pairs(src, X, Y, offset_rows=rows, stride=1, seed=k)
     assert rows > 10000
     net = Predictor(64, seed=0)
     net.fit_stats(X[:rows], Y[:rows])
@@ -138,12 +139,13 @@ def test_learned_step_keeps_fixed_point_and_cuts_iterations(pond):
     res = {}
     for learned in (False, True):
         with pond.Solver(lattice="D3Q27", shape=(n, n, n), precision="fp64", tau=0.52) as s:
-            s.set_state(rho, g, f=f)
+            s.copy_state_from(src)  # both time levels
             if learned:
                 attach(s, net, gate=0.0)
             s.step(1)
             d = s.diagnostics()
             res[learned] = (s.get_state(), d["niter_mean"], d["nonconverged"])
+    src.close()
     (fa, ra, ga), ia, nca = res[False]
     (fb, rb, gb), ib, ncb = res[True]
     assert nca == 0 and ncb == 0
