@@ -237,6 +237,57 @@ int pond_predict(pond_ctx* ctx, float* guess);
 int pond_step_noalloc(const pond_params* params, const float* f_in, const float* rho_in, const float* g_in,
                       float* f_out, float* rho_out, float* g_out, pond_diag* diag_out, void* stream);
 
+/* ---- Batched 1D mode.  No counterpart in the reference, which steps one
+   grid per process (lbm.cu:179-298); the per-node arithmetic is the D1Q5
+   step above (LBMpull, steps.cu:356-588), float32 populations with float64
+   moments and convergence test.
+
+   A batch holds independent D1Q5 problems of 1..4096 nodes each with
+   zero-gradient (clamped) ends.  Problems are packed into bins of up to 4096
+   nodes; one persistent kernel launch advances every bin K steps, each CTA
+   holding its bin in shared memory, and the launch sequence is captured once
+   in a CUDA graph and replayed.  Host arrays are float64 in the caller's
+   problem order, problems concatenated (f: 5 planes of pond_batch_nodes()). */
+typedef struct pond_batch pond_batch;
+/* interp: POND_WENO5 or POND_LAGR4; tau > 0.5 */
+int pond_batch_create(int nproblems, const int32_t* lengths, int interp, double tau, double tol_abs,
+                      double tol_rel, int max_iter, int device, pond_batch** out);
+int pond_batch_destroy(pond_batch* batch);
+int64_t pond_batch_nodes(const pond_batch* batch);
+int32_t pond_batch_bins(const pond_batch* batch);
+/* macroscopic state per node (rho, u finite, T > 0); populations become
+   w_i*rho in each node's own gauge; resets the step counter */
+int pond_batch_set_state(pond_batch* batch, const double* rho, const double* u, const double* T);
+/* any pointer may be NULL */
+int pond_batch_get_state(pond_batch* batch, double* f, double* rho, double* u, double* T);
+/* training pairs, written during pond_batch_run: every `every` steps (0 =
+   off) at local coordinates x % stride == 0, X[capacity][21] (device) gets
+   the pre-step rho, u, T at x-3..x+3 (clamped), Y[capacity][2] the converged
+   u, T of that step; rows in no particular order, the row count restarts at
+   0 with each call */
+int pond_batch_set_pairs(pond_batch* batch, float* X, float* Y, int64_t capacity, int every, int stride);
+int pond_batch_pairs_written(pond_batch* batch, int64_t* rows);
+/* advance every problem nsteps steps, k steps per persistent launch; *ms
+   (may be NULL) receives the device time of the call (CUDA events) */
+int pond_batch_run(pond_batch* batch, int nsteps, int k, float* ms);
+/* iteration statistics of the last pond_batch_run */
+int pond_batch_stats(pond_batch* batch, int64_t* niter_sum, int64_t* nonconverged, int32_t* niter_max);
+/* Tile of the persistent kernel: threads per CTA (256, 512, 768 or 1024)
+   and lane_cap, the iterations a node runs on one lane before it is handed
+   to a whole warp (>= 1; >= max_iter keeps every node on one lane). */
+int pond_batch_set_tile(pond_batch* batch, int threads, int lane_cap);
+int pond_batch_get_tile(const pond_batch* batch, int* threads, int* lane_cap);
+/* candidates of pond_batch_autotune: every thread count x lane_cap pair,
+   index = 4 * thread_index + cap_index */
+#define POND_BATCH_TILES 16
+static const int POND_BATCH_TILE_THREADS[4] = {256, 512, 768, 1024};
+static const int POND_BATCH_TILE_CAPS[4] = {4, 8, 16, 100};
+/* time probe_steps steps with each candidate tile on the current state,
+   keep the fastest, restore the state; ms_per_candidate: POND_BATCH_TILES
+   floats or NULL */
+int pond_batch_autotune(pond_batch* batch, int probe_steps, int* best_threads, int* best_lane_cap,
+                        float* ms_per_candidate);
+
 #ifdef __cplusplus
 }
 #endif

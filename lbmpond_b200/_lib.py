@@ -85,6 +85,22 @@ SIGNATURES = {
     "pond_set_predictor": (ctypes.c_int, [_vp, _vp, ctypes.c_float]),
     "pond_predict": (ctypes.c_int, [_vp, _vp]),
     "pond_set_extrapolation": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "pond_batch_create": (ctypes.c_int, [ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                         ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_vp)]),
+    "pond_batch_destroy": (ctypes.c_int, [_vp]),
+    "pond_batch_nodes": (ctypes.c_int64, [_vp]),
+    "pond_batch_bins": (ctypes.c_int32, [_vp]),
+    "pond_batch_set_state": (ctypes.c_int, [_vp, _dp, _dp, _dp]),
+    "pond_batch_get_state": (ctypes.c_int, [_vp, _dp, _dp, _dp, _dp]),
+    "pond_batch_set_pairs": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int64, ctypes.c_int, ctypes.c_int]),
+    "pond_batch_pairs_written": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int64)]),
+    "pond_batch_run": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]),
+    "pond_batch_stats": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
+                                        _i32p]),
+    "pond_batch_set_tile": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
+    "pond_batch_get_tile": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "pond_batch_autotune": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                           ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float)]),
 }
 
 _lib = None

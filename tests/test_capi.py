@@ -34,7 +34,7 @@ def test_binding_covers_header(pond):
     from lbmpond_b200 import _lib
     declared = set(header_functions())
     bound = set(_lib.SIGNATURES)
-    assert declared <= bound | {n for n in declared if n.startswith(("pond_mlp", "pond_batch", "pond_pred"))}
+    assert declared <= bound, sorted(declared - bound)
 
 
 def test_params_default_and_strings(pond):
@@ -89,3 +89,44 @@ def test_arr_roundtrip(tmp_path, pond):
     assert shape == (4, 3, 2) and np.array_equal(back, data)
     raw = np.fromfile(p, dtype=np.int32, count=6)
     assert raw.tolist() == [0, 3, 8, 4, 3, 2]  # drop.cu:12-20 header
+
+
+@pytest.mark.parametrize("lengths,interp,tau,status", [
+    ([10, 0, 5], 8, 0.9, -1),      # empty problem
+    ([10, 4097], 8, 0.9, -1),      # longer than a bin
+    ([], 8, 0.9, -1),              # no problems
+    ([10, 20], 7, 0.9, -5),        # TVD is not built for the batch
+    ([10, 20], 8, 0.5, -1),        # BGK needs tau > 0.5
+])
+def test_batch_create_validates_before_device(pond, lengths, interp, tau, status):
+    from lbmpond_b200 import _lib
+    L = _lib.load()
+    arr = (ctypes.c_int32 * max(len(lengths), 1))(*lengths)
+    h = ctypes.c_void_p()
+    assert L.pond_batch_create(len(lengths), arr, interp, tau, 1e-7, 1e-6, 100, 0, ctypes.byref(h)) == status
+    assert not h.value
+    assert L.pond_last_error_string().decode()
+    assert L.pond_batch_destroy(None) == 0
+    assert L.pond_batch_run(None, 1, 1, None) == -1
+    assert L.pond_batch_nodes(None) == 0
+
+
+def test_riemann_problem_set():
+    import numpy as np
+    from lbmpond_b200.batch import riemann_problems
+    lengths, rho, u, T = riemann_problems(4096, seed=0)
+    assert lengths.size == 4096 and lengths.min() >= 256 and lengths.max() <= 4096
+    assert rho.size == u.size == T.size == int(lengths.sum())
+    assert 1500 < lengths.mean() < 2900
+    p = rho * T
+    assert rho.min() >= 0.1 - 1e-12 and rho.max() <= 10 + 1e-9
+    assert p.min() >= 0.1 - 1e-12 and p.max() <= 10 + 1e-9
+    assert np.abs(u).max() <= 1
+    # two constant states per problem, the jump at the midpoint
+    off = np.concatenate([[0], np.cumsum(lengths)])
+    for q in (0, 17, 4095):
+        r = rho[off[q]:off[q + 1]]
+        n = lengths[q]
+        assert np.all(r[:n // 2] == r[0]) and np.all(r[n // 2:] == r[-1])
+    again = riemann_problems(4096, seed=0)
+    assert np.array_equal(again[0], lengths) and np.array_equal(again[3], T)
