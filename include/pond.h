@@ -277,16 +277,11 @@ int pond_batch_stats(pond_batch* batch, int64_t* niter_sum, int64_t* nonconverge
    to a whole warp (>= 1; >= max_iter keeps every node on one lane). */
 int pond_batch_set_tile(pond_batch* batch, int threads, int lane_cap);
 int pond_batch_get_tile(const pond_batch* batch, int* threads, int* lane_cap);
-/* candidates of pond_batch_autotune: every thread count x lane_cap pair,
-   index = 4 * thread_index + cap_index */
-#define POND_BATCH_TILES 16
-static const int POND_BATCH_TILE_THREADS[4] = {256, 512, 768, 1024};
-static const int POND_BATCH_TILE_CAPS[4] = {4, 8, 16, 100};
-/* time probe_steps steps with each candidate tile on the current state,
-   keep the fastest, restore the state; ms_per_candidate: POND_BATCH_TILES
-   floats or NULL */
-int pond_batch_autotune(pond_batch* batch, int probe_steps, int* best_threads, int* best_lane_cap,
-                        float* ms_per_candidate);
+/* time probe_steps steps with each of ncand candidate tiles (int32 pairs
+   threads, lane_cap) on the current state, keep the fastest, restore the
+   state; ms_out (ncand floats) and best (its index) may be NULL */
+int pond_batch_autotune(pond_batch* batch, int probe_steps, const int32_t* tiles, int ncand, float* ms_out,
+                        int* best);
 
 #ifdef __cplusplus
 }

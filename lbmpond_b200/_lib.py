@@ -99,8 +99,8 @@ SIGNATURES = {
                                         _i32p]),
     "pond_batch_set_tile": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
     "pond_batch_get_tile": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
-    "pond_batch_autotune": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
-                                           ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float)]),
+    "pond_batch_autotune": (ctypes.c_int, [_vp, ctypes.c_int, _i32p, ctypes.c_int, ctypes.POINTER(ctypes.c_float),
+                                           ctypes.POINTER(ctypes.c_int)]),
 }
 
 _lib = None

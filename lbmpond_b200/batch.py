@@ -17,9 +17,8 @@ from . import _lib
 from ._lib import LAGR4, WENO5
 
 NPAIR_IN, NPAIR_OUT = 21, 2
-THREAD_CHOICES = (256, 512, 768, 1024)
-LANE_CAPS = (4, 8, 16, 100)
-TILES = tuple((t, c) for t in THREAD_CHOICES for c in LANE_CAPS)  # order of pond_batch_autotune
+# autotuner candidates: (threads per CTA, lane_cap)
+TILES = tuple((t, c) for t in (256, 512, 768, 1024) for c in (2, 4, 8, 16)) + ((768, 100),)
 
 
 def _dp(a):
@@ -137,9 +136,12 @@ class Batch:
     def tile(self, tc):
         _lib.check(self._L.pond_batch_set_tile(self._h, int(tc[0]), int(tc[1])))
 
-    def autotune(self, probe_steps=10):
-        """Pick the fastest tile; returns ((threads, lane_cap), {tile: ms})."""
-        t, c = ctypes.c_int(), ctypes.c_int()
-        ms = (ctypes.c_float * len(TILES))()
-        _lib.check(self._L.pond_batch_autotune(self._h, int(probe_steps), ctypes.byref(t), ctypes.byref(c), ms))
-        return (int(t.value), int(c.value)), dict(zip(TILES, [float(v) for v in ms]))
+    def autotune(self, probe_steps=10, tiles=TILES):
+        """Pick the fastest tile; returns (tile, {tile: ms})."""
+        cand = np.ascontiguousarray(np.asarray(tiles, np.int32).reshape(-1, 2))
+        ms = (ctypes.c_float * len(cand))()
+        best = ctypes.c_int()
+        _lib.check(self._L.pond_batch_autotune(self._h, int(probe_steps),
+                                               cand.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), len(cand), ms,
+                                               ctypes.byref(best)))
+        return tuple(int(v) for v in cand[best.value]), {tuple(int(v) for v in t): float(m) for t, m in zip(cand, ms)}

@@ -146,10 +146,11 @@ __device__ __forceinline__ float weno5(const float w[5], float d) {
   const float b0 = beta_js(w[0], w[1], w[2], 1.f, -4.f, 3.f);
   const float b1 = beta_js(w[1], w[2], w[3], 1.f, 0.f, -1.f);
   const float b2 = beta_js(w[2], w[3], w[4], 3.f, -4.f, 1.f);
-  const float a0 = d0 / ((1e-6f + b0) * (1e-6f + b0));
-  const float a1 = d1 / ((1e-6f + b1) * (1e-6f + b1));
-  const float a2 = d2 / ((1e-6f + b2) * (1e-6f + b2));
-  return (a0 * S[0] + a1 * S[1] + a2 * S[2]) / (a0 + a1 + a2);
+  // the nonlinear weights only scale the candidates: 2-ulp divisions
+  const float a0 = __fdividef(d0, (1e-6f + b0) * (1e-6f + b0));
+  const float a1 = __fdividef(d1, (1e-6f + b1) * (1e-6f + b1));
+  const float a2 = __fdividef(d2, (1e-6f + b2) * (1e-6f + b2));
+  return __fdividef(a0 * S[0] + a1 * S[1] + a2 * S[2], a0 + a1 + a2);
 }
 
 // cubic Lagrange weights (propagate<4>) at offset t in [1, 2) from the first
@@ -203,7 +204,11 @@ __device__ __forceinline__ bool moments_and_test(const Args& a, const float fn[5
     const double fv = fn[k];
     rho += fv; m1 += fv * vk[k]; m2 += fv * vk[k] * vk[k];
   }
-  if (rho != 0) { m1 /= rho; m2 /= rho; }
+  if (rho != 0) {
+    const double ir = 1.0 / rho;
+    m1 *= ir;
+    m2 *= ir;
+  }
   double Tn = m2 - m1 * m1;
   if (Tn < 0) Tn = s.T;
   bool ok = !(fabs(m1 - s.U) >= a.tol_abs + a.tol_rel * fabs(m1)) &&
@@ -330,7 +335,7 @@ __global__ void __launch_bounds__(NT, 1) batch_kernel(Args a) {
       while (s.x < fill) {
         s.niter++;
         const double C = sqrt(s.T / L::TLat);
-        const float Uf = float(s.U), invC = float(1.0 / C);
+        const float Uf = float(s.U), invC = __frcp_rn(float(C));
         double vk[5];
         float fn[5];
 #pragma unroll
@@ -373,7 +378,7 @@ __global__ void __launch_bounds__(NT, 1) batch_kernel(Args a) {
         while (w.niter < a.max_iter) {
           w.niter++;
           const double C = sqrt(w.T / L::TLat);
-          const float Uf = float(w.U), invC = float(1.0 / C);
+          const float Uf = float(w.U), invC = __frcp_rn(float(C));
           double vk[5];
 #pragma unroll
           for (int j = 0; j < 5; j++) vk[j] = C * L::xi1(j) + w.U;
@@ -436,7 +441,7 @@ struct pond_batch {
   double tau = 0.9, tol_abs = 1e-7, tol_rel = 1e-6;
   int max_iter = 100;
   int threads = 768;   // threads per CTA (autotuned)
-  int lane_cap = 8;    // phase-1 iterations per node (autotuned)
+  int lane_cap = 4;    // phase-1 iterations per node (autotuned)
   int grid = 0;
   cudaStream_t stream = nullptr;
   float* f = nullptr;
@@ -798,9 +803,13 @@ int pond_batch_get_tile(const pond_batch* b, int* threads, int* lane_cap) {
   return POND_OK;
 }
 
-int pond_batch_autotune(pond_batch* b, int probe_steps, int* best_threads, int* best_lane_cap,
-                        float* ms_per_candidate) {
-  if (!b || probe_steps < 1) return set_error(POND_ERR_ARG, "pond_batch_autotune: bad argument");
+int pond_batch_autotune(pond_batch* b, int probe_steps, const int32_t* tiles, int ncand, float* ms_out, int* best) {
+  if (!b || probe_steps < 1 || !tiles || ncand < 1) return set_error(POND_ERR_ARG, "pond_batch_autotune: bad argument");
+  for (int c = 0; c < ncand; c++) {
+    const int t = tiles[2 * c], l = tiles[2 * c + 1];
+    if ((t != 256 && t != 512 && t != 768 && t != 1024) || l < 1)
+      return set_error(POND_ERR_ARG, "autotune candidate %d is not a valid tile", c);
+  }
   cudaSetDevice(b->device);
   const long long n = b->Ltot;
   float* snap = nullptr;
@@ -817,22 +826,21 @@ int pond_batch_autotune(pond_batch* b, int probe_steps, int* best_threads, int* 
   if (e == cudaSuccess) e = cudaMemcpy(&istep_dev, b->istep_dev, sizeof(int), cudaMemcpyDeviceToHost);
   for (int i = 0; i < 4 && e == cudaSuccess; i++)
     e = cudaMemcpyAsync(snap + at[i], parts[i], cnt[i] * sizeof(float), cudaMemcpyDeviceToDevice, b->stream);
-  const int saved_every = b->pair_every, saved_threads = b->threads, saved_cap = b->lane_cap;
+  const int saved_every = b->pair_every, saved[2] = {b->threads, b->lane_cap};
   b->pair_every = 0;
   batch::drop_graph(b);
-  float best = 1e30f;
-  int best_t = saved_threads, best_c = saved_cap;
+  float best_ms = 1e30f;
+  int best_c = -1;
   int st = e == cudaSuccess ? POND_OK : cuda_fail(e, "autotune snapshot");
-  for (int c = 0; c < POND_BATCH_TILES && st == POND_OK; c++) {
-    b->threads = POND_BATCH_TILE_THREADS[c / 4];
-    b->lane_cap = POND_BATCH_TILE_CAPS[c % 4];
+  for (int c = 0; c < ncand && st == POND_OK; c++) {
+    b->threads = tiles[2 * c];
+    b->lane_cap = tiles[2 * c + 1];
     float ms = 0;
     st = pond_batch_run(b, probe_steps, probe_steps, &ms);
-    if (ms_per_candidate) ms_per_candidate[c] = ms;
-    if (st == POND_OK && ms < best) {
-      best = ms;
-      best_t = b->threads;
-      best_c = b->lane_cap;
+    if (ms_out) ms_out[c] = ms;
+    if (st == POND_OK && ms < best_ms) {
+      best_ms = ms;
+      best_c = c;
     }
     for (int i = 0; i < 4 && st == POND_OK; i++) {
       e = cudaMemcpyAsync(parts[i], snap + at[i], cnt[i] * sizeof(float), cudaMemcpyDeviceToDevice, b->stream);
@@ -848,11 +856,11 @@ int pond_batch_autotune(pond_batch* b, int probe_steps, int* best_threads, int* 
   cudaStreamSynchronize(b->stream);
   cudaFree(snap);
   b->pair_every = saved_every;
-  b->threads = st == POND_OK ? best_t : saved_threads;
-  b->lane_cap = st == POND_OK ? best_c : saved_cap;
+  const bool ok = st == POND_OK && best_c >= 0;
+  b->threads = ok ? tiles[2 * best_c] : saved[0];
+  b->lane_cap = ok ? tiles[2 * best_c + 1] : saved[1];
   batch::drop_graph(b);
-  if (best_threads) *best_threads = b->threads;
-  if (best_lane_cap) *best_lane_cap = b->lane_cap;
+  if (best) *best = best_c;
   return st;
 }
 

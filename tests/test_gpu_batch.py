@@ -162,14 +162,15 @@ def test_training_pairs(pond):
 
 
 def test_autotune_restores_state(pond):
-    from lbmpond_b200.batch import TILES, Batch
+    from lbmpond_b200.batch import Batch
     lengths = [4096, 2000, 3000, 1000, 512]
     rho, u, T = _mild_problems(lengths, seed=2)
     with Batch(lengths, interp=WENO5) as b:
         b.set_state(rho, u, T)
         before = b.get_state()
-        best, ms = b.autotune(probe_steps=2)
-        assert best in TILES and b.tile == best
+        tiles = [(512, 4), (768, 4), (1024, 2), (256, 100)]
+        best, ms = b.autotune(probe_steps=2, tiles=tiles)
+        assert best in tiles and b.tile == best and len(ms) == len(tiles)
         assert all(v > 0 for v in ms.values())
         after = b.get_state()
         for x, y in zip(before, after):
@@ -182,4 +183,24 @@ def test_autotune_restores_state(pond):
         c.run(2)
         ref = c.get_state()
     for x, y in zip(stepped, ref):  # same arithmetic, other register allocation
+        assert np.abs(x - y).max() <= 1e-6 * np.abs(y).max()
+
+
+@pytest.mark.parametrize("tile", [(256, 1), (512, 2), (1024, 3), (768, 100)])
+def test_tiles_agree(pond, tile):
+    """Every tile computes the same step: the lane cap only moves iterations
+    between one lane and a warp."""
+    from lbmpond_b200.batch import Batch
+    lengths = [4096, 1800, 2100, 35]
+    rho, u, T = _mild_problems(lengths, seed=9, width=0)  # sharp jumps: many parked nodes
+    res = []
+    for t in ((512, 100), tile):
+        with Batch(lengths, interp=WENO5, tau=0.6) as b:
+            b.tile = t
+            b.set_state(rho, u, T)
+            b.run(3)
+            res.append((b.get_state(), b.stats()))
+    (sa, ta), (sb, tb) = res
+    assert ta["niter_sum"] == tb["niter_sum"] and ta["nonconverged"] == tb["nonconverged"]
+    for x, y in zip(sa, sb):
         assert np.abs(x - y).max() <= 1e-6 * np.abs(y).max()
