@@ -391,6 +391,42 @@ def run_ours(args, rank, local, world, pg):
     return out
 
 
+def run_batch1d(steps=1000, nproblems=4096):
+    """The batched D1Q5 workload: `nproblems` seeded Riemann problems
+    (lengths uniform in [256, 4096], rho and p log-uniform in [0.1, 10], u
+    uniform in [-1, 1], jump at the midpoint), WENO5, tau 0.9, float32 with
+    float64 moments, `steps` steps in persistent graph-replayed launches of
+    50 steps after the autotuner picked the tile.  Reported beside the
+    D3Q27 line; problems whose state became non-finite are counted (the
+    float64 oracle diverges on the same strong-jump problems)."""
+    from lbmpond_b200.batch import Batch, riemann_problems
+    import torch
+    lengths, rho, u, T = riemann_problems(nproblems, seed=0)
+    with Batch(lengths, interp=8, tau=0.9) as b:
+        b.set_state(rho, u, T)
+        tile, _ = b.autotune(probe_steps=5)
+        b.set_state(rho, u, T)
+        ms = b.run(steps, steps_per_launch=50)
+        st = b.stats()
+        f, r, uu, tt = b.get_state()
+        fin = np.isfinite(f).all(0) & np.isfinite(r) & np.isfinite(uu) & np.isfinite(tt)
+        bad = int(sum(not fin[b.offsets[p]:b.offsets[p + 1]].all() for p in range(nproblems)))
+        cap = 1 << 21
+        X = torch.empty((cap, 21), dtype=torch.float32, device="cuda")
+        Y = torch.empty((cap, 2), dtype=torch.float32, device="cuda")
+        b.set_state(rho, u, T)
+        b.set_pairs(X, Y, every=10, stride=16)
+        ms_pairs = b.run(100, steps_per_launch=50)
+        pairs = b.pairs_written()
+        nodes = b.nodes
+    return {"workload": f"{nproblems} D1Q5 Riemann problems, lengths U[256,4096] (seed 0), WENO5, {steps} steps",
+            "nodes": nodes, "MLUPS": nodes * steps / (ms / 1e3) / 1e6, "ms_per_step": ms / steps,
+            "tile": {"threads": tile[0], "lane_cap": tile[1]}, "niter_mean": st["niter_sum"] / (nodes * steps),
+            "nonconverged_frac": st["nonconverged"] / (nodes * steps), "nonfinite_problems": bad,
+            "pairs": {"rows_per_100_steps": pairs, "every": 10, "stride": 16,
+                      "ms_per_step_with_pairs": ms_pairs / 100}}
+
+
 def run_reference(args, rank, world):
     """The reference arm: the reference's step restated on the host (FP64
     oracle; the reference itself has no CPU implementation), all host threads,
@@ -438,6 +474,11 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ref-cuda", action="store_true", help="also time the reference's own kernels (64^3)")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched 1D measurement")
+    ap.add_argument("--batch-steps", type=int, default=1000)
+    ap.add_argument("--batch-problems", type=int, default=4096)
+    ap.add_argument("--workload", default="d3q27", choices=["d3q27", "batch1d"],
+                    help="batch1d: only the batched D1Q5 measurement (one JSON object)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -448,12 +489,18 @@ def main():
             return
         print(json.dumps(run_reference(args, rank, world)), flush=True)
         return
+    if args.workload == "batch1d":
+        if int(os.environ.get("RANK", "0")) == 0:
+            print(json.dumps(run_batch1d(args.batch_steps, args.batch_problems)), flush=True)
+        return
     rank, local, world, pg = dist_setup(args.gpus)
     out = run_ours(args, rank, local, world, pg)
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline()
     if rank == 0 and args.ref_cuda:
         out["reference_cuda"] = reference_cuda()
+    if rank == 0 and world == 1 and not args.no_batch:
+        out["batch1d"] = run_batch1d(args.batch_steps, args.batch_problems)
     if pg is not None:
         pg.barrier()
         pg.destroy_process_group()
