@@ -427,6 +427,102 @@ def run_batch1d(steps=1000, nproblems=4096):
                       "ms_per_step_with_pairs": ms_pairs / 100}}
 
 
+def _time_steps(s, steps, warmup):
+    s.step(warmup)
+    ms = []
+    for _ in range(steps):
+        s.step(1)
+        ms.append(s.last_step_ms())
+    return float(np.mean(ms)), s.diagnostics()
+
+
+def shock_vortex_state(n, mach=1.5, T1=0.1, eps=0.3, radius=0.05, gamma=5.0 / 3.0):
+    """Stationary normal shock at x = 0.5 (pre-shock rho = 1, T = T1, flow
+    along +x at `mach`; post-shock state from the Rankine-Hugoniot
+    relations) and an isentropic vortex of strength `eps` (velocity scale
+    eps * c1) and radius `radius` at (0.25, 0.5) in x, y on the unit box, in
+    lattice units of the D3Q125 gauge (TLat = 1).  gamma = 5/3 is the
+    monatomic 3D gas the step models."""
+    x = (np.arange(n) + 0.5) / n
+    X, Y, _ = np.meshgrid(x, x, x, indexing="ij")  # [x, y, z]
+    c1 = np.sqrt(gamma * T1)
+    u1 = mach * c1
+    r21 = (gamma + 1) * mach ** 2 / ((gamma - 1) * mach ** 2 + 2)
+    p21 = 1 + 2 * gamma / (gamma + 1) * (mach ** 2 - 1)
+    pre = X < 0.5
+    dx, dy = X - 0.25, Y - 0.5
+    e = np.exp(0.5 * (1 - (dx * dx + dy * dy) / radius ** 2)) * pre
+    ux = np.where(pre, u1, u1 / r21) - eps * c1 * dy / radius * e
+    uy = eps * c1 * dx / radius * e
+    T = np.where(pre, T1, T1 * p21 / r21) * (1 - (gamma - 1) / 2 * eps ** 2 * e * e)
+    rho = np.where(pre, (1 - (gamma - 1) / 2 * eps ** 2 * e * e) ** (1 / (gamma - 1)), r21)
+    flat = lambda a: np.ascontiguousarray(a.transpose(2, 1, 0)).ravel()  # x fastest
+    return flat(rho), np.stack([flat(ux), flat(uy), np.zeros(n ** 3), flat(T)])
+
+
+def run_configs(steps=5, warmup=2, d3q125_size=48):
+    """Step throughput of the other workloads: the D1Q5 Sod tube (float64,
+    TVD, checked against the float64 oracle over the full 500 steps), the
+    D3Q27 Taylor-Green vortex at 128^3 (quadratic, float32) and the D3Q125
+    shock-vortex box (fixed-origin quadratic, float32).  Progress goes to
+    stderr."""
+    import lbmpond_b200 as pond
+    out = {}
+    t_start = time.perf_counter()
+
+    def note(msg):
+        print(f"[configs {time.perf_counter() - t_start:7.1f} s] {msg}", file=sys.stderr, flush=True)
+
+    # config 1: 1000 nodes on [0,1], dt/dx = 0.1 -> T = 0.01 p/rho (at dt/dx >= 0.2 the
+    # TVD iteration of the float64 oracle itself goes non-finite within 20 steps)
+    n, lam2 = 1000, 0.01
+    left, right = (1.0, 0.0, lam2 * 1.0), (0.125, 0.0, lam2 * 0.1 / 0.125)
+    with pond.Solver(lattice="D1Q5", shape=(n, 1, 1), precision="fp64", interp=pond.TVD, tau=0.55,
+                     bc=("clamp",) * 3) as s:
+        s.init("sod", 0.5, *left, *right)
+        f0, r0, g0 = s.get_state()
+        t0 = time.perf_counter()
+        s.step(500)
+        wall = time.perf_counter() - t0
+        f1, r1, g1 = s.get_state()
+        d = s.diagnostics()
+    note("sod: GPU done")
+    from oracle import oracle as O  # the float64 oracle is the checker of this row
+    st = O.State(f0, r0, g0)
+    for _ in range(500):
+        st, _, _ = O.step(st, 0, (n, 1, 1), interp=7, tau=0.55, bc=(1, 1, 1))
+    note("sod: oracle done")
+    out["sod_d1q5_fp64"] = {"workload": "D1Q5 Sod, 1000 nodes, TVD, tau 0.55, zero-gradient ends, 500 steps, float64",
+                            "ms_per_step_wall": wall / 500 * 1e3,
+                            "max_rel_diff_vs_oracle": {"rho": float(np.abs(r1 - st.rho).max() / np.abs(st.rho).max()),
+                                                       "T": float(np.abs(g1[3] - st.g[3]).max() / np.abs(st.g[3]).max())},
+                            "niter_max_last_step": d["niter_max"]}
+    # config 2: TGV 128^3, Mach 0.5 with gamma 5/3, T0 = TLat/4 (c = 0.5 node/step)
+    T0 = (1.0 / 3.0) / 4
+    U0 = 0.5 * np.sqrt(5.0 / 3.0 * T0)
+    with pond.Solver(lattice="D3Q27", shape=(128,) * 3, precision="fp32", interp=pond.LAGR3, tau=0.51) as s:
+        s.init("tgv", U0, T0, 1.0, 5.0 / 3.0)
+        ms, d = _time_steps(s, steps, warmup)
+        out["tgv_d3q27_128"] = {"workload": "D3Q27 Taylor-Green 128^3, Mach 0.5, quadratic Lagrange, tau 0.51, float32",
+                                "ms_per_step": ms, "MLUPS": 128 ** 3 / ms / 1e3, "niter_mean": d["niter_mean"],
+                                "niter_max": d["niter_max"], "steps_timed": f"{warmup + 1}..{warmup + steps}"}
+    note("tgv done")
+    # config 5: D3Q125 shock + vortex
+    m = d3q125_size
+    with pond.Solver(lattice="D3Q125", shape=(m,) * 3, precision="fp32", tau=0.9,
+                     bc=("clamp", "periodic", "periodic")) as s:
+        rho, g = shock_vortex_state(m)
+        s.set_state(rho, g)
+        note(f"d3q125 {m}^3 state set")
+        ms, d = _time_steps(s, max(1, steps // 2), 1)
+        note("d3q125 done")
+        out["shock_vortex_d3q125"] = {"workload": f"D3Q125 {m}^3 Mach 1.5 shock + isentropic vortex, fixed-origin "
+                                                  "quadratic, zero-gradient x ends, periodic y/z, float32",
+                                      "ms_per_step": ms, "MLUPS": m ** 3 / ms / 1e3, "niter_mean": d["niter_mean"],
+                                      "niter_max": d["niter_max"], "nonconverged": d["nonconverged"]}
+    return out
+
+
 def run_reference(args, rank, world):
     """The reference arm: the reference's step restated on the host (FP64
     oracle; the reference itself has no CPU implementation), all host threads,
@@ -477,8 +573,9 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched 1D measurement")
     ap.add_argument("--batch-steps", type=int, default=1000)
     ap.add_argument("--batch-problems", type=int, default=4096)
-    ap.add_argument("--workload", default="d3q27", choices=["d3q27", "batch1d"],
-                    help="batch1d: only the batched D1Q5 measurement (one JSON object)")
+    ap.add_argument("--workload", default="d3q27", choices=["d3q27", "batch1d", "configs"],
+                    help="batch1d: only the batched D1Q5 measurement; configs: the other workloads (one JSON object)")
+    ap.add_argument("--d3q125-size", type=int, default=48)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -492,6 +589,10 @@ def main():
     if args.workload == "batch1d":
         if int(os.environ.get("RANK", "0")) == 0:
             print(json.dumps(run_batch1d(args.batch_steps, args.batch_problems)), flush=True)
+        return
+    if args.workload == "configs":
+        if int(os.environ.get("RANK", "0")) == 0:
+            print(json.dumps(run_configs(args.steps, args.warmup, args.d3q125_size)), flush=True)
         return
     rank, local, world, pg = dist_setup(args.gpus)
     out = run_ours(args, rank, local, world, pg)
