@@ -8,6 +8,7 @@
 #include "pond_internal.h"
 #include "pond_step_1d.cuh"
 #include "pond_step_d3q125.cuh"
+#include "pond_step_d3q125_tile.cuh"
 #include "pond_step_d3q27.cuh"
 #include "pond_step_point.cuh"
 
@@ -218,6 +219,15 @@ template <typename R> static int launch_typed(pond_ctx* c) {
       }
       break;
     case POND_D3Q125: {
+      if constexpr (std::is_same<R, float>::value) {
+        const size_t smem = sizeof(d125t::Smem);
+        e = cudaFuncSetAttribute(d125t::pull_d3q125_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+        const dim3 grd((a.nx + d125t::T - 1) / d125t::T, (a.ny + d125t::T - 1) / d125t::T,
+                       (a.nz + d125t::T - 1) / d125t::T);
+        d125t::pull_d3q125_tile_kernel<<<grd, d125t::THREADS, smem, s>>>(a);
+        break;
+      }
       const size_t smem = sizeof(D125Smem<R>);
       e = cudaFuncSetAttribute(pull_d3q125_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");

@@ -74,6 +74,7 @@ CASES = [
     (1, (6, 6, 6), 2),
     (1, (6, 5, 6), 5),
     (2, (5, 4, 4), 6),
+    (2, (9, 6, 5), 6),    # several 4x4x4 tiles, ragged in every axis
 ]
 
 
