@@ -6,7 +6,7 @@
 // float64 moments and convergence test), organised for the SM:
 //
 //  * a CTA owns a 4 x 4 x 4 tile and stages it with its +-1 halo (6 x 6 x 6
-//    nodes: 125 population planes, the gauge velocities and c, 114 KB) once
+//    nodes: 125 population planes, the gauge velocities and c, 113 KB) once
 //    per step, so two CTAs fit on an SM and every staged node serves up to
 //    27 centres from shared memory;
 //  * each of the 8 warps takes 8 nodes of the tile in turn and iterates one
@@ -40,23 +40,38 @@ struct Smem {
   float f[125 * PS];       // staged populations, non-finite values zeroed
   float u[3][SN];          // staged velocities (sign-flipped on mirrored axes)
   float c[SN];             // sqrts(T / TLat)
-  int gidx[SN];            // global node of each staged node
   unsigned char flags[SN]; // mirrored axes (bits 0-2)
-  float M[WARPS][3][5][5]; // per-warp weighted basis rows of the current stencil node
+  float M[WARPS][3][6][5]; // per-warp weighted basis rows of the current stencil node (row 5: idle lanes)
 };
 
-// Row i of the 5-point Lagrange basis on {0, +EC1, -EC1, +EC2, -EC2} at y:
-// L_i(y) = D_i (y^2 - P_i)(y^2 + s_i y - Q_i)
-__device__ __forceinline__ float basis5(int i, float y) {
-  constexpr double e1s = EC1 * EC1, e2s = EC2 * EC2;
-  const float D = i == 0 ? float(1.0 / (e1s * e2s))
-                         : (i <= 2 ? float(1.0 / (2.0 * e1s * (e1s - e2s))) : float(1.0 / (2.0 * e2s * (e2s - e1s))));
-  const float P = (i == 1 || i == 2) ? float(e2s) : float(e1s);
-  const float s = i == 1 ? float(EC1) : i == 2 ? -float(EC1) : i == 3 ? float(EC2) : i == 4 ? -float(EC2) : 0.f;
-  const float Q = i == 0 ? float(e2s) : 0.f;
-  const float y2 = y * y;
-  return D * (y2 - P) * (fmaf(s, y, y2) - Q);
+static_assert(2 * (sizeof(Smem) + 1024) <= 233472, "two CTAs must fit in the 228 KB of an SM");
+
+// global node of staged node i and its mirror flags
+__device__ __forceinline__ int staged_global(const StepArgs<float>& a, int x0, int y0, int z0, int i, bool rv[3]) {
+  const int hx = i % S, hy = (i / S) % S, hz = i / (S * S);
+  const int gx = resolve_axis(x0 - 1 + hx, a.nx, a.bc[0], rv[0]);
+  const int gy = resolve_axis(y0 - 1 + hy, a.ny, a.bc[1], rv[1]);
+  const int gz = resolve_axis(z0 - 1 + hz, a.nz, a.bc[2], rv[2]);
+  return gx + a.nx * (gy + a.ny * gz);
 }
+
+// Row i of the 5-point Lagrange basis on {0, +EC1, -EC1, +EC2, -EC2}:
+// L_i(y) = D_i (y^2 - P_i)(y^2 + s_i y - Q_i), coefficients per row
+struct BasisRow {
+  float D, P, s, Q;
+  __device__ __forceinline__ explicit BasisRow(int i) {
+    constexpr double e1s = EC1 * EC1, e2s = EC2 * EC2;
+    D = i == 0 ? float(1.0 / (e1s * e2s))
+               : (i <= 2 ? float(1.0 / (2.0 * e1s * (e1s - e2s))) : float(1.0 / (2.0 * e2s * (e2s - e1s))));
+    P = (i == 1 || i == 2) ? float(e2s) : float(e1s);
+    s = i == 1 ? float(EC1) : i == 2 ? -float(EC1) : i == 3 ? float(EC2) : i == 4 ? -float(EC2) : 0.f;
+    Q = i == 0 ? float(e2s) : 0.f;
+  }
+  __device__ __forceinline__ float operator()(float y) const {
+    const float y2 = y * y;
+    return D * (y2 - P) * (fmaf(s, y, y2) - Q);
+  }
+};
 
 __device__ __forceinline__ double xi5(int c) { return Lattice<POND_D3Q125>::xi1(c); }
 
@@ -70,12 +85,7 @@ __global__ void __launch_bounds__(THREADS, 2) pull_d3q125_tile_kernel(StepArgs<f
   // ---- stage the tile (steps.cu:164-193 per node, once per CTA here)
   for (int i = tid; i < SN; i += THREADS) {
     bool rv[3];
-    const int hx = i % S, hy = (i / S) % S, hz = i / (S * S);
-    const int gx = resolve_axis(x0 - 1 + hx, a.nx, a.bc[0], rv[0]);
-    const int gy = resolve_axis(y0 - 1 + hy, a.ny, a.bc[1], rv[1]);
-    const int gz = resolve_axis(z0 - 1 + hz, a.nz, a.bc[2], rv[2]);
-    const int g = gx + a.nx * (gy + a.ny * gz);
-    sm.gidx[i] = g;
+    const int g = staged_global(a, x0, y0, z0, i, rv);
     sm.flags[i] = (unsigned char)((rv[0] ? 1 : 0) | (rv[1] ? 2 : 0) | (rv[2] ? 4 : 0));
 #pragma unroll
     for (int k = 0; k < 3; k++) {
@@ -85,11 +95,12 @@ __global__ void __launch_bounds__(THREADS, 2) pull_d3q125_tile_kernel(StepArgs<f
     const float Tn = a.g_in[3 * a.N + g];
     sm.c[i] = copysignf(sqrtf(fabsf(Tn) * float(1.0 / L::TLat)), Tn);
   }
-  __syncthreads();
   for (int idx = tid; idx < 125 * SN; idx += THREADS) {
     const int p = idx / SN, i = idx - p * SN;
+    bool rv[3];
+    const int g = staged_global(a, x0, y0, z0, i, rv);
     const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(&sm.f[p * PS + i]));
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(a.f_in + (long long)p * a.N + sm.gidx[i])
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(a.f_in + (long long)p * a.N + g)
                  : "memory");
   }
   asm volatile("cp.async.wait_all;\n" ::: "memory");
@@ -102,8 +113,11 @@ __global__ void __launch_bounds__(THREADS, 2) pull_d3q125_tile_kernel(StepArgs<f
   __syncthreads();
 
   // ---- one warp per node; lane 5j+k: source / target x-class j, z-class k
+  // idle lanes (25..31) compute like lane 20+k and write table row 5, which nobody reads
   const bool worker = lane < 25;
-  const int j = worker ? lane / 5 : 4, k = lane % 5;
+  const int j = worker ? lane / 5 : 4, k = lane % 5, jrow = worker ? j : 5;
+  const BasisRow Lj(j);
+  const float xik = float(xi5(k));
   NodeSums ns = {0, 0, 0, 0, 0, 0, 0ull, 0ull, 0ull, 0};
   for (int t = warp; t < T * T * T; t += WARPS) {
     const int lx = t % T, ly = (t / T) % T, lz = t / (T * T);
@@ -150,26 +164,29 @@ __global__ void __launch_bounds__(THREADS, 2) pull_d3q125_tile_kernel(StepArgs<f
         const int na[3] = {n / 9, (n / 3) % 3, n % 3};
         const int q = qc + (na[2] - 1) * S * S + (na[1] - 1) * S + (na[0] - 1);
         // this lane's three basis entries M[ax][j][k] = w_j L_j(s + r xi_k)
-        if (worker) {
-          const float cq = sm.c[q];
+        {
+          const float cq = sm.c[q] * invC;
           const unsigned fl = sm.flags[q];
 #pragma unroll
           for (int ax = 0; ax < 3; ax++) {
             const float s = (sm.u[ax][q] - Uf[ax]) * invC;
-            const float r = ((fl >> ax) & 1 ? -cq : cq) * invC;
+            const float r = (fl >> ax) & 1 ? -cq : cq;
             const float wj = na[ax] == 0 ? w3[ax][0] : na[ax] == 1 ? w3[ax][1] : w3[ax][2];
-            sm.M[warp][ax][j][k] = wj * finite_or_zero_f(basis5(j, fmaf(r, float(xi5(k)), s)));
+            sm.M[warp][ax][jrow][k] = wj * finite_or_zero_f(Lj(fmaf(r, xik, s)));
           }
         }
         __syncwarp();
         // z pass: t1[jy] = sum_jz Mz[k][jz] f[j][jy][jz]
+        float mz[5];
+#pragma unroll
+        for (int jz = 0; jz < 5; jz++) mz[jz] = sm.M[warp][2][k][jz];
         float t1[5];
         const float* fq = sm.f + (25 * j) * PS + q;
 #pragma unroll
         for (int jy = 0; jy < 5; jy++) {
           float v = 0.f;
 #pragma unroll
-          for (int jz = 0; jz < 5; jz++) v += sm.M[warp][2][k][jz] * fq[(5 * jy + jz) * PS];
+          for (int jz = 0; jz < 5; jz++) v += mz[jz] * fq[(5 * jy + jz) * PS];
           t1[jy] = v;
         }
         // y pass: t2[iy] = sum_jy My[iy][jy] t1[jy]
@@ -182,9 +199,12 @@ __global__ void __launch_bounds__(THREADS, 2) pull_d3q125_tile_kernel(StepArgs<f
           t2[iy] = v;
         }
         // x pass: acc[iy] += sum_jx Mx[j][jx] t2 of lane (jx, k)
+        float mxr[5];
+#pragma unroll
+        for (int jx = 0; jx < 5; jx++) mxr[jx] = sm.M[warp][0][j][jx];
 #pragma unroll
         for (int jx = 0; jx < 5; jx++) {
-          const float mx = sm.M[warp][0][j][jx];
+          const float mx = mxr[jx];
 #pragma unroll
           for (int iy = 0; iy < 5; iy++) acc[iy] += mx * __shfl_sync(0xffffffffu, t2[iy], 5 * jx + k);
         }
