@@ -507,19 +507,49 @@ def run_configs(steps=5, warmup=2, d3q125_size=48):
                                 "ms_per_step": ms, "MLUPS": 128 ** 3 / ms / 1e3, "niter_mean": d["niter_mean"],
                                 "niter_max": d["niter_max"], "steps_timed": f"{warmup + 1}..{warmup + steps}"}
     note("tgv done")
-    # config 5: D3Q125 shock + vortex
+    # config 5: D3Q125 shock + vortex, plain and learned start from the same spun-up state
+    import torch
+    from lbmpond_b200.learned import Predictor, attach, calibrate_gate, collect_pairs, keep_history
     m = d3q125_size
-    with pond.Solver(lattice="D3Q125", shape=(m,) * 3, precision="fp32", tau=0.9,
-                     bc=("clamp", "periodic", "periodic")) as s:
+    kw = dict(lattice="D3Q125", shape=(m,) * 3, precision="fp32", tau=0.9, bc=("clamp", "periodic", "periodic"))
+    with pond.Solver(**kw) as s, pond.Solver(**kw) as snap:
         rho, g = shock_vortex_state(m)
         s.set_state(rho, g)
         note(f"d3q125 {m}^3 state set")
-        ms, d = _time_steps(s, max(1, steps // 2), 1)
-        note("d3q125 done")
-        out["shock_vortex_d3q125"] = {"workload": f"D3Q125 {m}^3 Mach 1.5 shock + isentropic vortex, fixed-origin "
-                                                  "quadratic, zero-gradient x ends, periodic y/z, float32",
-                                      "ms_per_step": ms, "MLUPS": m ** 3 / ms / 1e3, "niter_mean": d["niter_mean"],
-                                      "niter_max": d["niter_max"], "nonconverged": d["nonconverged"]}
+        cap = 2_000_000
+        X = torch.zeros((cap, 39), dtype=torch.float32, device="cuda")
+        Y = torch.zeros((cap, 4), dtype=torch.float32, device="cuda")
+        rows = 0
+        keep_history(s, True)
+        for k in range(8):
+            s.step(1)
+            rows += collect_pairs(s, X, Y, offset_rows=rows, stride=31, seed=k)
+        keep_history(s, False)
+        snap.copy_state_from(s)
+        ms_p, d_p = _time_steps(s, max(1, steps // 2), 1)
+        _, rho_p, _ = s.get_state()
+        note("d3q125 plain timed")
+        net = Predictor(128, seed=0)
+        net.fit_stats(X[:rows], Y[:rows])
+        loss = net.train(X[:rows], Y[:rows], steps=2000, batch=8192, lr=2e-3)
+        gate, _ = calibrate_gate(net, X[:rows], Y[:rows])
+        s.copy_state_from(snap)
+        attach(s, net, gate=gate)
+        ms_l, d_l = _time_steps(s, max(1, steps // 2), 1)
+        _, rho_l, _ = s.get_state()
+        attach(s, None)
+        net.close()
+        note("d3q125 learned timed")
+        out["shock_vortex_d3q125"] = {
+            "workload": f"D3Q125 {m}^3 Mach 1.5 shock + isentropic vortex, fixed-origin quadratic, zero-gradient x "
+                        "ends, periodic y/z, float32; 8 spin-up steps feed the training pairs",
+            "plain": {"ms_per_step": ms_p, "MLUPS": m ** 3 / ms_p / 1e3, "niter_mean": d_p["niter_mean"],
+                      "niter_max": d_p["niter_max"], "nonconverged": d_p["nonconverged"]},
+            "learned": {"ms_per_step": ms_l, "MLUPS": m ** 3 / ms_l / 1e3, "niter_mean": d_l["niter_mean"],
+                        "niter_max": d_l["niter_max"], "nonconverged": d_l["nonconverged"],
+                        "network": "39-128-128-4", "pairs": rows, "loss_first": float(loss[0]),
+                        "loss_last": float(loss[-1]), "gate": gate},
+            "l1_rho_learned_vs_plain": float(np.abs(rho_l - rho_p).mean() / np.abs(rho_p).mean())}
     return out
 
 

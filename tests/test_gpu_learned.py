@@ -153,3 +153,44 @@ def test_learned_step_keeps_fixed_point_and_cuts_iterations(pond):
     assert np.abs(ga[3] - gb[3]).max() <= 1e-8 * np.abs(ga[3]).max()
     assert ib < ia, (ia, ib)
     net.close()
+
+
+def test_learned_start_on_d3q125(pond):
+    """The predictor is lattice-generic: on a D3Q125 blast (float64, the
+    width-128 network of the D3Q125 workload) the learned start reaches the
+    plain step's fixed point."""
+    torch = _torch()
+    from lbmpond_b200.learned import Predictor, attach, collect_pairs, keep_history
+    n = 12
+    sphere = (0.5, 0.5, 0.5, 0.25, 1.0, 0.1, 0.3, 0.06)
+    cap = 200000
+    X = torch.zeros((cap, M.NIN), dtype=torch.float32, device="cuda")
+    Y = torch.zeros((cap, M.NOUT), dtype=torch.float32, device="cuda")
+    rows = 0
+    src = pond.Solver(lattice="D3Q125", shape=(n, n, n), precision="fp64", tau=0.6)
+    src.init("sphere", *sphere)
+    keep_history(src)
+    for k in range(12):
+        src.step(1)
+        rows += collect_pairs(src, X, Y, offset_rows=rows, stride=1, seed=k)
+    assert rows > 2000
+    net = Predictor(128, seed=0)
+    net.fit_stats(X[:rows], Y[:rows])
+    loss = net.train(X[:rows], Y[:rows], steps=800, batch=2048, lr=2e-3)
+    assert loss[-50:].mean() < loss[:10].mean()
+    res = {}
+    for learned in (False, True):
+        with pond.Solver(lattice="D3Q125", shape=(n, n, n), precision="fp64", tau=0.6) as s:
+            s.copy_state_from(src)
+            if learned:
+                attach(s, net, gate=0.0)
+            s.step(1)
+            d = s.diagnostics()
+            res[learned] = (s.get_state(), d["niter_mean"], d["nonconverged"])
+    src.close()
+    (fa, ra, ga), ia, nca = res[False]
+    (fb, rb, gb), ib, ncb = res[True]
+    assert nca == 0 and ncb == 0
+    assert np.abs(fa - fb).max() <= 1e-8 * np.abs(fa).max()
+    assert np.abs(ga[3] - gb[3]).max() <= 1e-8 * np.abs(ga[3]).max()
+    net.close()
