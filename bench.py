@@ -296,12 +296,19 @@ def run_ours(args, rank, local, world, pg):
     # reference-precision result) against the float32 plain and learned paths
     l1 = None
     if not args.no_l1 and world == 1:
+        def drift(obj, d0):
+            d1 = obj.diagnostics()
+            return {"mass": (d1["mass"] - d0["mass"]) / d0["mass"] / args.l1_steps,
+                    "energy": (d1["enrg"] - d0["enrg"]) / d0["enrg"] / args.l1_steps}
+
         ref64 = mk("fp64")
         ref64.copy_state_from(snap)
+        d0 = ref64.diagnostics()
         ref64.step(args.l1_steps)
         fr = ref64.fields()
+        l1 = {"steps": args.l1_steps, "reference": "float64 GPU path (tolerance 1e-12 + 1e-10|v|)",
+              "drift_per_step": {"fp64": drift(ref64, d0)}}
         ref64.close()
-        l1 = {"steps": args.l1_steps, "reference": "float64 GPU path (tolerance 1e-12 + 1e-10|v|)"}
         for name, use in (("plain", None), ("learned", net)):
             if name == "learned" and net is None:
                 continue
@@ -309,8 +316,10 @@ def run_ours(args, rank, local, world, pg):
             t.copy_state_from(snap)
             if use is not None:
                 attach(t, use, gate=learned["training"]["gate"])
+            d0 = t.diagnostics()
             t.step(args.l1_steps)
             ft = t.fields()
+            l1["drift_per_step"][name] = drift(t, d0)
             t.close()
             l1[name] = {"rho": _l1(ft["rho"], fr["rho"]), "T": _l1(ft["T"], fr["T"])}
 
