@@ -323,8 +323,11 @@ def run_ours(args, rank, local, world, pg):
             t.close()
             l1[name] = {"rho": _l1(ft["rho"], fr["rho"]), "T": _l1(ft["T"], fr["T"])}
 
-    # e2e through the C ABI with host buffers on the timed path: upload the
-    # state from pinned host memory, step, read back rho/u/T (drop() fields)
+    # e2e through the C ABI with host buffers on the timed path: every step
+    # uploads its full input state from pinned host memory and reads rho, u, T
+    # (the drop() fields) back, through pond_step_host, which overlaps one
+    # step's copies with the neighbouring steps on two copy streams.  Timed by
+    # the host clock between synchronisations (what a caller observes).
     e2e = None
     if not args.no_e2e:
         f_h = torch.empty((27, N), dtype=torch.float32, pin_memory=True)
@@ -333,24 +336,22 @@ def run_ours(args, rank, local, world, pg):
         s.download_native(f_h.data_ptr(), r_h.data_ptr(), g_h.data_ptr())
         ro_h = torch.empty(N, dtype=torch.float32, pin_memory=True)
         go_h = torch.empty((4, N), dtype=torch.float32, pin_memory=True)
-        stream = torch.cuda.ExternalStream(s.stream(), device=local)
-        k = max(1, min(args.steps, 5))
-        s.upload_native(f_h.data_ptr(), r_h.data_ptr(), g_h.data_ptr())
-        s.step(1)
-        s.download_native(None, ro_h.data_ptr(), go_h.data_ptr())
+        attach(s, None)  # the pipelined call runs the plain start
+        k = max(3, min(args.steps, 8))
+        io = (f_h.data_ptr(), r_h.data_ptr(), g_h.data_ptr(), ro_h.data_ptr(), go_h.data_ptr())
+        for _ in range(2):
+            s.step_host(*io)
+        s.sync()
         barrier(pg)
         torch.cuda.synchronize()
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ev0.record(stream)
+        t0 = time.perf_counter()
         for _ in range(k):
-            s.upload_native(f_h.data_ptr(), r_h.data_ptr(), g_h.data_ptr())
-            s.step(1)
-            s.download_native(None, ro_h.data_ptr(), go_h.data_ptr())
-        ev1.record(stream)
-        ev1.synchronize()
-        e2e_ms = allmax(pg, ev0.elapsed_time(ev1) / k)
-        e2e = {"value": world * N / (e2e_ms / 1e3) / 1e6, "unit": "MLUPS", "path": path,
-               "h2d_bytes_per_step": (27 + 5) * N * 4, "d2h_bytes_per_step": 5 * N * 4, "ms_per_step": e2e_ms}
+            s.step_host(*io)
+        s.sync()
+        e2e_ms = allmax(pg, (time.perf_counter() - t0) * 1e3 / k)
+        e2e = {"value": world * N / (e2e_ms / 1e3) / 1e6, "unit": "MLUPS", "path": "plain (pond_step_host)",
+               "h2d_bytes_per_step": (27 + 5) * N * 4, "d2h_bytes_per_step": 5 * N * 4, "ms_per_step": e2e_ms,
+               "steps": k, "timing": "host clock around the calls, synchronised on both sides"}
 
     achieved_gbs = BYTES_PER_NODE * N / (ms_step / 1e3) / 1e9
     peaks = {}

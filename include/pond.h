@@ -237,6 +237,25 @@ int pond_predict(pond_ctx* ctx, float* guess);
 int pond_step_noalloc(const pond_params* params, const float* f_in, const float* rho_in, const float* g_in,
                       float* f_out, float* rho_out, float* g_out, pond_diag* diag_out, void* stream);
 
+/* Pipelined step from host buffers.  No counterpart in the reference, whose
+   state never leaves the device; this is calcStep plus the two PCIe copies a
+   caller with host-resident states would otherwise issue around it.
+
+   Queues the copy of an input state (f[Q*N], rho[N], g[4*N] in the
+   context's precision, pinned host memory for full PCIe speed) to the
+   device, one plain step from it (no predictor: POND_ERR_STATE while one is
+   bound), and the copy of the result's rho and g to rho_out / g_out (either
+   may be NULL); returns without waiting.  Uploads and read-backs run on two
+   copy streams of the context, so consecutive calls overlap their copies with
+   the neighbouring steps.  The host buffers of a call must stay untouched
+   until pond_sync; the last result is the context's current state.  Any
+   other call on the context waits for the queued work first.  The first call
+   allocates two input slots of one state each on the device. */
+int pond_step_host(pond_ctx* ctx, const void* f_in, const void* rho_in, const void* g_in, void* rho_out,
+                   void* g_out);
+/* wait for all queued pond_step_host work */
+int pond_sync(pond_ctx* ctx);
+
 /* ---- Batched 1D mode.  No counterpart in the reference, which steps one
    grid per process (lbm.cu:179-298); the per-node arithmetic is the D1Q5
    step above (LBMpull, steps.cu:356-588), float32 populations with float64

@@ -166,6 +166,18 @@ class Solver:
         vp = lambda a: ctypes.c_void_p(a) if a else None  # noqa: E731
         _lib.check(self._L.pond_download_state(self._ctx, vp(f), vp(rho), vp(g)))
 
+    def step_host(self, f, rho, g, rho_out=None, g_out=None):
+        """Queue one plain step from host buffers in the context's precision
+        (addresses of pinned arrays, as upload_native) and the read-back of the
+        result's rho and g; returns at once.  Copies overlap neighbouring calls'
+        steps.  The buffers must stay untouched until sync()."""
+        vp = lambda a: ctypes.c_void_p(a) if a else None  # noqa: E731
+        _lib.check(self._L.pond_step_host(self._ctx, vp(f), vp(rho), vp(g), vp(rho_out), vp(g_out)))
+
+    def sync(self):
+        """Wait for every queued step_host call."""
+        _lib.check(self._L.pond_sync(self._ctx))
+
     def copy_state_from(self, other: "Solver"):
         """Device-side copy of another context's current state (precision converted)."""
         _lib.check(self._L.pond_copy_state(self._ctx, other._ctx))

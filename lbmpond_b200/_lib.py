@@ -85,6 +85,8 @@ SIGNATURES = {
     "pond_set_predictor": (ctypes.c_int, [_vp, _vp, ctypes.c_float]),
     "pond_predict": (ctypes.c_int, [_vp, _vp]),
     "pond_set_extrapolation": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "pond_step_host": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "pond_sync": (ctypes.c_int, [_vp]),
     "pond_batch_create": (ctypes.c_int, [ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                          ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_vp)]),
     "pond_batch_destroy": (ctypes.c_int, [_vp]),

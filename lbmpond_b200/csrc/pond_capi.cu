@@ -246,6 +246,7 @@ void* pond_stream(pond_ctx* c) { return c ? (void*)c->stream : nullptr; }
 
 int pond_device_state(pond_ctx* c, void** f, void** rho, void** g) {
   if (!c) return set_error(POND_ERR_ARG, "null context");
+  { const int ps = pipe_drain(c); if (ps != POND_OK) return ps; }
   if (f) *f = c->f[c->cur];
   if (rho) *rho = c->rho[c->cur];
   if (g) *g = c->g[c->cur];
@@ -254,6 +255,7 @@ int pond_device_state(pond_ctx* c, void** f, void** rho, void** g) {
 
 int pond_init(pond_ctx* c, int ic, const double* prm, int nprm) {
   if (!c) return set_error(POND_ERR_ARG, "null context");
+  { const int ps = pipe_drain(c); if (ps != POND_OK) return ps; }
   if (ic < POND_IC_ACOUSTIC || ic > POND_IC_UNIFORM) return set_error(POND_ERR_ARG, "unknown initial condition %d", ic);
   if (nprm < 0 || nprm > 8 || (nprm > 0 && !prm)) return set_error(POND_ERR_ARG, "bad initial-condition parameters");
   cudaSetDevice(c->p.device);
@@ -296,6 +298,7 @@ int pond_init(pond_ctx* c, int ic, const double* prm, int nprm) {
 
 int pond_set_state(pond_ctx* c, const double* f, const double* rho, const double* g) {
   if (!c || !rho || !g) return set_error(POND_ERR_ARG, "pond_set_state: null argument");
+  { const int ps = pipe_drain(c); if (ps != POND_OK) return ps; }
   cudaSetDevice(c->p.device);
   const long long N = c->N;
   const int Q = c->Q;
@@ -329,6 +332,7 @@ int pond_set_state(pond_ctx* c, const double* f, const double* rho, const double
 
 int pond_get_state(pond_ctx* c, double* f, double* rho, double* g) {
   if (!c) return set_error(POND_ERR_ARG, "null context");
+  { const int ps = pipe_drain(c); if (ps != POND_OK) return ps; }
   if (!c->initialized) return set_error(POND_ERR_STATE, "state not initialised");
   cudaSetDevice(c->p.device);
   int st = POND_OK;
@@ -340,6 +344,7 @@ int pond_get_state(pond_ctx* c, double* f, double* rho, double* g) {
 
 int pond_get_fields(pond_ctx* c, double* rho, double* ux, double* uy, double* uz, double* T) {
   if (!c) return set_error(POND_ERR_ARG, "null context");
+  { const int ps = pipe_drain(c); if (ps != POND_OK) return ps; }
   if (!c->initialized) return set_error(POND_ERR_STATE, "state not initialised");
   cudaSetDevice(c->p.device);
   int st = POND_OK;
@@ -390,6 +395,7 @@ int pond_get_niter(pond_ctx* c, int32_t* out) {
 
 int pond_step(pond_ctx* c, int nsteps) {
   if (!c) return set_error(POND_ERR_ARG, "null context");
+  { const int ps = pipe_drain(c); if (ps != POND_OK) return ps; }
   if (nsteps < 0) return set_error(POND_ERR_ARG, "nsteps < 0");
   if (!c->initialized) return set_error(POND_ERR_STATE, "pond_step before pond_init/pond_set_state");
   if (c->p.learned && !c->guess_ready) return set_error(POND_ERR_STATE, "learned step without a predictor");
@@ -425,6 +431,7 @@ int pond_last_step_ms(pond_ctx* c, float* ms) {
 
 int pond_upload_state(pond_ctx* c, const void* f, const void* rho, const void* g) {
   if (!c || !f || !rho || !g) return set_error(POND_ERR_ARG, "pond_upload_state: null argument");
+  { const int ps = pipe_drain(c); if (ps != POND_OK) return ps; }
   cudaSetDevice(c->p.device);
   const size_t N = (size_t)c->N;
   cudaError_t e = cudaMemcpyAsync(c->f[c->cur], f, (size_t)c->Q * N * c->elem, cudaMemcpyHostToDevice, c->stream);
@@ -438,6 +445,7 @@ int pond_upload_state(pond_ctx* c, const void* f, const void* rho, const void* g
 
 int pond_download_state(pond_ctx* c, void* f, void* rho, void* g) {
   if (!c) return set_error(POND_ERR_ARG, "null context");
+  { const int ps = pipe_drain(c); if (ps != POND_OK) return ps; }
   if (!c->initialized) return set_error(POND_ERR_STATE, "state not initialised");
   cudaSetDevice(c->p.device);
   const size_t N = (size_t)c->N;
@@ -463,6 +471,7 @@ extern "C" {
 
 int pond_copy_state(pond_ctx* dst, pond_ctx* src) {
   if (!dst || !src) return set_error(POND_ERR_ARG, "null context");
+  for (pond_ctx* x : {dst, src}) { const int ps = pipe_drain(x); if (ps != POND_OK) return ps; }
   if (dst->p.lattice != src->p.lattice || dst->N != src->N || dst->p.Nx != src->p.Nx || dst->p.Ny != src->p.Ny)
     return set_error(POND_ERR_ARG, "pond_copy_state: lattice or grid differ");
   if (dst->p.device != src->p.device) return set_error(POND_ERR_ARG, "pond_copy_state: contexts on different devices");
@@ -507,6 +516,7 @@ int pond_last_step_work(pond_ctx* c, int64_t* work) {
 
 int pond_diagnostics(pond_ctx* c, pond_diag* out) {
   if (!c || !out) return set_error(POND_ERR_ARG, "null argument");
+  { const int ps = pipe_drain(c); if (ps != POND_OK) return ps; }
   cudaSetDevice(c->p.device);
   cudaError_t e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_fail(e, "pond_diagnostics");

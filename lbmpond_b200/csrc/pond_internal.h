@@ -33,6 +33,15 @@ struct pond_ctx {
   double curtime = 0;
   void* staging = nullptr;  // pinned host staging for conversions
   size_t staging_bytes = 0;
+  // host-buffer pipeline (pond_step_host): two input slots, copy streams, events
+  void* in_f[2] = {nullptr, nullptr};
+  void* in_rho[2] = {nullptr, nullptr};
+  void* in_g[2] = {nullptr, nullptr};
+  cudaStream_t h2d = nullptr, d2h = nullptr;
+  cudaEvent_t ev_in_ready[2] = {nullptr, nullptr}, ev_step_done[2] = {nullptr, nullptr},
+              ev_out_free[2] = {nullptr, nullptr};
+  long long pipe_k = 0;
+  bool pipe_pending = false;
 };
 
 namespace pond {
@@ -49,6 +58,11 @@ void ctx_free(pond_ctx* c);
 int upload(pond_ctx* c, const double* src, size_t count, void* dst);
 int download(pond_ctx* c, const void* src, size_t count, double* dst);
 int launch_step(pond_ctx* c);
+// one plain step between explicit device buffers {f, rho, g} (no predictor)
+int launch_step_io(pond_ctx* c, const void* const in[3], void* const out[3]);
+// wait for the host-buffer pipeline (pond_step_host) if one is in flight
+int pipe_drain(pond_ctx* c);
+void pipe_free(pond_ctx* c);
 int state_sums(pond_ctx* c, pond_diag* out);
 // learned path: run the bound predictor on the current state into c->guess
 int run_predictor(pond_ctx* c);

@@ -699,6 +699,7 @@ int pond_collect_pairs(pond_ctx* c, float* X, float* Y, int64_t* node, int64_t c
                        uint64_t seed, int64_t* written) {
   if (!c || !X || !Y || capacity <= 0 || stride <= 0 || !written)
     return set_error(POND_ERR_ARG, "pond_collect_pairs: bad argument");
+  { const int ps = pipe_drain(c); if (ps != POND_OK) return ps; }
   if (c->istep < 1) return set_error(POND_ERR_STATE, "pond_collect_pairs needs a completed step");
   if (!c->g_hist || !c->keep_history)
     return set_error(POND_ERR_STATE, "pond_collect_pairs needs pond_keep_history(ctx, 1) before the step");
@@ -753,6 +754,7 @@ int pond_set_extrapolation(pond_ctx* c, int on) {
 
 int pond_predict(pond_ctx* c, float* guess_out) {
   if (!c || !guess_out) return set_error(POND_ERR_ARG, "null argument");
+  { const int ps = pipe_drain(c); if (ps != POND_OK) return ps; }
   if (!c->initialized) return set_error(POND_ERR_STATE, "state not initialised");
   cudaSetDevice(c->p.device);
   int st = run_predictor(c);

@@ -37,6 +37,7 @@ int ctx_alloc(pond_ctx* c) {
 }
 
 void ctx_free(pond_ctx* c) {
+  pipe_free(c);
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (int b = 0; b < 2; b++) {
     cudaFree(c->f[b]); cudaFree(c->rho[b]); cudaFree(c->g[b]);
@@ -162,12 +163,19 @@ template <int LAT, int N, typename R> static void launch_point(const StepArgs<R>
   }
 }
 
-template <typename R> static int launch_typed(pond_ctx* c) {
+// One step from in[] = {f, rho, g} to out[] (device buffers of the context's
+// precision); with in == nullptr the context's own double buffer is used.
+template <typename R> static int launch_typed(pond_ctx* c, const void* const* in = nullptr, void* const* out = nullptr) {
   StepArgs<R> a;
   const int i = c->cur, o = 1 - c->cur;
-  a.f_in = (const R*)c->f[i]; a.rho_in = (const R*)c->rho[i]; a.g_in = (const R*)c->g[i];
-  a.f_out = (R*)c->f[o]; a.rho_out = (R*)c->rho[o]; a.g_out = (R*)c->g[o];
-  a.guess = c->p.learned ? c->guess : nullptr;
+  if (in) {
+    a.f_in = (const R*)in[0]; a.rho_in = (const R*)in[1]; a.g_in = (const R*)in[2];
+    a.f_out = (R*)out[0]; a.rho_out = (R*)out[1]; a.g_out = (R*)out[2];
+  } else {
+    a.f_in = (const R*)c->f[i]; a.rho_in = (const R*)c->rho[i]; a.g_in = (const R*)c->g[i];
+    a.f_out = (R*)c->f[o]; a.rho_out = (R*)c->rho[o]; a.g_out = (R*)c->g[o];
+  }
+  a.guess = (c->p.learned && !in) ? c->guess : nullptr;
   a.niter_out = c->keep_niter ? c->niter : nullptr;
   a.sums = c->d_sums;
   a.nx = (int)c->p.Nx; a.ny = (int)c->p.Ny; a.nz = (int)c->p.Nz;
@@ -239,6 +247,10 @@ template <typename R> static int launch_typed(pond_ctx* c) {
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "step kernel launch");
   return POND_OK;
+}
+
+int launch_step_io(pond_ctx* c, const void* const in[3], void* const out[3]) {
+  return c->elem == 8 ? launch_typed<double>(c, in, out) : launch_typed<float>(c, in, out);
 }
 
 int launch_step(pond_ctx* c) {

@@ -130,3 +130,10 @@ def test_riemann_problem_set():
         assert np.all(r[:n // 2] == r[0]) and np.all(r[n // 2:] == r[-1])
     again = riemann_problems(4096, seed=0)
     assert np.array_equal(again[0], lengths) and np.array_equal(again[3], T)
+
+
+def test_step_host_validates_before_device(pond):
+    from lbmpond_b200 import _lib
+    L = _lib.load()
+    assert L.pond_step_host(None, None, None, None, None, None) == -1
+    assert L.pond_sync(None) == -1
