@@ -145,26 +145,34 @@ def allmax(pg, v):
 
 
 # ------------------------------------------------------------------ CPU baseline (oracle)
-def cpu_baseline(budget_s=15.0):
-    """FP64 oracle (restated reference step) on a bounded sample of the same
-    initial condition, all host threads."""
+def _oracle_sample(m, spin, warmup, steps):
+    """The FP64 oracle (restated reference step, all host threads) on an m^3
+    sample of the sphere problem: `spin` + `warmup` untimed steps (spin = the
+    benchmark's spin-up scaled to the sample, so the blast has crossed the
+    same fraction of the box), then `steps` timed steps."""
     from oracle import oracle as O
     O.build()
-    n = 12
-    st = O.base_state(1, *sphere_state(n)[:1], *sphere_state(n)[1])
-    t0 = time.perf_counter()
-    O.step(st, 1, (n, n, n), tau=TAU, tol_abs=TOL_ABS, tol_rel=TOL_REL)
-    dt = time.perf_counter() - t0
-    # grow the sample to use about budget_s of CPU time
-    per_node = dt / n ** 3
-    m = int(max(n, min(40, round((budget_s / per_node) ** (1 / 3)))))
     rho, g = sphere_state(m)
     st = O.base_state(1, rho, *g)
+    for _ in range(spin + warmup):
+        st, _, _ = O.step(st, 1, (m, m, m), tau=TAU, tol_abs=TOL_ABS, tol_rel=TOL_REL)
     t0 = time.perf_counter()
-    O.step(st, 1, (m, m, m), tau=TAU, tol_abs=TOL_ABS, tol_rel=TOL_REL)
-    dt = time.perf_counter() - t0
-    return {"value": m ** 3 / dt / 1e6, "unit": "MLUPS", "cores": O.max_threads(), "kind": "port",
-            "sample": f"one step of the same sphere problem at {m}^3 on the FP64 oracle ({dt:.1f} s)"}
+    it = []
+    for _ in range(steps):
+        st, niter, _ = O.step(st, 1, (m, m, m), tau=TAU, tol_abs=TOL_ABS, tol_rel=TOL_REL)
+        it.append(float(niter.mean()))
+    dt = (time.perf_counter() - t0) / steps
+    return m ** 3 / dt / 1e6, dt, float(np.mean(it)), O.max_threads()
+
+
+def cpu_baseline(spinup=150, m=24):
+    """FP64 oracle on a bounded sample of the same problem at the same stage
+    of the blast (about 10-30 s of host time)."""
+    spin = round(spinup * m / 256)
+    v, dt, it, cores = _oracle_sample(m, spin, 0, 2)
+    return {"value": v, "unit": "MLUPS", "cores": cores, "kind": "port",
+            "sample": f"{m}^3 sample of the sphere problem after {spin} spin-up steps (the 256^3 spin-up scaled), "
+                      f"2 timed steps of {dt:.2f} s on the FP64 oracle, {it:.2f} iterations per node"}
 
 
 # ------------------------------------------------------------------ reference kernels on the GPU
@@ -566,28 +574,19 @@ def run_configs(steps=5, warmup=2, d3q125_size=48):
 def run_reference(args, rank, world):
     """The reference arm: the reference's step restated on the host (FP64
     oracle; the reference itself has no CPU implementation), all host threads,
-    each step a bounded sample of the same problem."""
-    from oracle import oracle as O
-    O.build()
+    each step a bounded sample of the same problem at the same stage of the
+    blast as the timed GPU steps."""
     m = args.ref_size
-    rho, g = sphere_state(m)
-    st0 = O.base_state(1, rho, *g)
-    for _ in range(args.warmup):
-        O.step(st0, 1, (m, m, m), tau=TAU, tol_abs=TOL_ABS, tol_rel=TOL_REL)
-    t0 = time.perf_counter()
-    st = st0
-    for _ in range(args.steps):
-        st, niter, _ = O.step(st, 1, (m, m, m), tau=TAU, tol_abs=TOL_ABS, tol_rel=TOL_REL)
-    dt = (time.perf_counter() - t0) / args.steps
-    v = m ** 3 / dt / 1e6
-    sample = f"{m}^3 sample of the sphere problem per step (FP64 oracle, {O.max_threads()} threads)"
+    spin = round(args.spinup * m / 256)
+    v, dt, it, cores = _oracle_sample(m, spin, args.warmup, args.steps)
+    sample = (f"{m}^3 sample of the sphere problem after {spin} spin-up steps (the 256^3 spin-up scaled), "
+              f"FP64 oracle, {cores} threads, {it:.2f} iterations per node")
     return {"impl": "reference", "metric": METRIC, "value": v, "unit": "MLUPS", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"D3Q27 spherical Riemann problem (sample {m}^3), tau {TAU}, cubic Lagrange",
                        "path": "reference step on the host"},
-            "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": O.max_threads(), "kind": "port",
-                             "sample": sample},
+            "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -606,7 +605,7 @@ def main():
     ap.add_argument("--train-steps", type=int, default=3000)
     ap.add_argument("--no-l1", action="store_true")
     ap.add_argument("--l1-steps", type=int, default=3)
-    ap.add_argument("--ref-size", type=int, default=12)
+    ap.add_argument("--ref-size", type=int, default=24)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ref-cuda", action="store_true", help="also time the reference's own kernels (64^3)")
@@ -637,7 +636,7 @@ def main():
     rank, local, world, pg = dist_setup(args.gpus)
     out = run_ours(args, rank, local, world, pg)
     if rank == 0 and world == 1 and not args.no_cpu:
-        out["cpu_baseline"] = cpu_baseline()
+        out["cpu_baseline"] = cpu_baseline(args.spinup)
     if rank == 0 and args.ref_cuda:
         out["reference_cuda"] = reference_cuda()
     if rank == 0 and world == 1 and not args.no_batch:
