@@ -234,12 +234,12 @@ template <typename R> static int launch_typed(pond_ctx* c, const void* const* in
         const dim3 grd((a.nx + d125t::T - 1) / d125t::T, (a.ny + d125t::T - 1) / d125t::T,
                        (a.nz + d125t::T - 1) / d125t::T);
         d125t::pull_d3q125_tile_kernel<<<grd, d125t::THREADS, smem, s>>>(a);
-        break;
+      } else {  // float64: one CTA per node, as the reference kernel
+        const size_t smem = sizeof(D125Smem<R>);
+        e = cudaFuncSetAttribute(pull_d3q125_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+        pull_d3q125_kernel<R><<<(unsigned)c->N, D125_THREADS, smem, s>>>(a);
       }
-      const size_t smem = sizeof(D125Smem<R>);
-      e = cudaFuncSetAttribute(pull_d3q125_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
-      pull_d3q125_kernel<R><<<(unsigned)c->N, D125_THREADS, smem, s>>>(a);
       break;
     }
     default: return set_error(POND_ERR_UNSUPPORTED, "lattice");
