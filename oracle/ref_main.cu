@@ -106,7 +106,7 @@ int main(int argc, char** argv) {
   parsHost.nFunc = 0;
   parsHost.Nx = LSizeX * brick.x; parsHost.Ny = LSizeY * brick.y; parsHost.Nz = LSizeZ * brick.z;
   if (parsHost.Nx != n[0] || parsHost.Ny != n[1] || parsHost.Nz != n[2]) {
-    fprintf(stderr, "state is %ldx%ldx%ld but this build is %ldx%ldx%ld\n", (long)n[0], (long)n[1], (long)n[2],
+    fprintf(stderr, "state is %ldx%ldx%ld but the binary was compiled for %ldx%ldx%ld\n", (long)n[0], (long)n[1], (long)n[2],
             parsHost.Nx, parsHost.Ny, parsHost.Nz);
     return 4;
   }
