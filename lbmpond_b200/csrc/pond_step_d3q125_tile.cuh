@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(THREADS, 2) pull_d3q125_tile_kernel(StepArgs<f
     while (niter < a.max_iter) {
       niter++;
       const double C = sqrt(Tc / L::TLat);
-      const float invC = float(1.0 / C);
+      const float invC = __frcp_rn(float(C));
       // LagrPol<3> factors of target class j (this lane's basis row) per
       // axis at the three stencil positions: shift = crd - (coord - 1)
       float w3[3][3];
@@ -227,9 +227,11 @@ __global__ void __launch_bounds__(THREADS, 2) pull_d3q125_tile_kernel(StepArgs<f
         for (int m = 0; m < 5; m++) mv[m] += __shfl_xor_sync(0xffffffffu, mv[m], o);
       const double rho = mv[0];
       double m[4] = {mv[1], mv[2], mv[3], mv[4]};
-      if (rho != 0)
+      if (rho != 0) {
+        const double ir = 1.0 / rho;
 #pragma unroll
-        for (int q = 0; q < 4; q++) m[q] /= rho;
+        for (int q = 0; q < 4; q++) m[q] *= ir;
+      }
       double Tn = (m[3] - m[0] * m[0] - m[1] * m[1] - m[2] * m[2]) * (1.0 / L::Dim);
       if (Tn < 0) Tn = Tc;  // steps.cu:475
       bool ok = true;

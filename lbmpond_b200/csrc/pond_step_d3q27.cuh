@@ -278,7 +278,7 @@ __global__ void __launch_bounds__(THREADS, 1) pull_d3q27_tile_kernel(StepArgs<fl
   unsigned long long work = 0;
   while (__any_sync(0xffffffffu, !done)) {
     if (!done) niter++;
-    const double C = sqrt(T / L::TLat);
+    const double C = sqrt(T * (1.0 / L::TLat));
     // relative window origins and Lagrange weights per axis and class
     int ro[3][3];
     float wt[3][3][N];
@@ -296,7 +296,7 @@ __global__ void __launch_bounds__(THREADS, 1) pull_d3q27_tile_kernel(StepArgs<fl
       lo[ax] = min(ro[ax][0], min(ro[ax][1], ro[ax][2]));
       hi[ax] = max(ro[ax][0], max(ro[ax][1], ro[ax][2])) + N - 1;
     }
-    const float invC = float(1.0 / C);
+    const float invC = __frcp_rn(float(C));
     const float Us[3] = {float(U[0]) * invC, float(U[1]) * invC, float(U[2]) * invC};
     float acc[27];
 #pragma unroll
@@ -388,7 +388,7 @@ __global__ void __launch_bounds__(THREADS, 1) pull_d3q27_tile_kernel(StepArgs<fl
       }
     }
     if (!done) {
-      if (!(C > 0.0) || !(fabs(1.0 / C) <= 1.0e300)) {
+      if (!(C >= 1.0e-300)) {  // C <= 0, NaN, or 1/C beyond 1e300
         // target T = 0: every transfer term is non-finite and dropped (structs.cuh:542)
 #pragma unroll
         for (int t = 0; t < 27; t++) acc[t] = 0.f;

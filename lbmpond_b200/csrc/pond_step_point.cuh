@@ -25,14 +25,17 @@ __device__ __forceinline__ float finite_or_zero_f(float v) { return fabsf(v) <= 
 __device__ __forceinline__ double finite_or_zero_f(double v) { return fabs(v) <= 1.7976931348623157e308 ? v : 0.0; }
 
 // Lagrange interpolation weights on N nodes at offset s from the first node
-// (steps.cu:595-601 LagrPol per axis, :602-608 LinPol for N = 2).
+// (steps.cu:595-601 LagrPol per axis, :602-608 LinPol for N = 2).  The node
+// spacings j - p are compile-time constants, so each factor multiplies by a
+// folded reciprocal instead of dividing (within one float64 ulp of the
+// quotient; a float64 division is a long instruction sequence).
 template <int N, typename R> __device__ __forceinline__ void lagr_weights(double s, R w[N]) {
 #pragma unroll
   for (int j = 0; j < N; j++) {
     double a = 1.0;
 #pragma unroll
     for (int p = 0; p < N; p++)
-      if (p != j) a *= (s - p) / double(j - p);
+      if (p != j) a *= (s - p) * (1.0 / double(j - p));
     w[j] = R(a);
   }
 }
@@ -207,8 +210,9 @@ __device__ __forceinline__ bool moments_and_test(const StepArgs<R>& a, const R a
         }
   }
   if (rho != 0) {
+    const double ir = 1.0 / rho;
 #pragma unroll
-    for (int k = 0; k < 4; k++) m[k] /= rho;
+    for (int k = 0; k < 4; k++) m[k] *= ir;
   }
   double Tn = (m[3] - m[0] * m[0] - m[1] * m[1] - m[2] * m[2]) * (1.0 / L::Dim);
   if (Tn < 0) Tn = T;
