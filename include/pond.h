@@ -262,7 +262,7 @@ int pond_sync(pond_ctx* ctx);
    moments and convergence test.
 
    A batch holds independent D1Q5 problems of 1..4096 nodes each with
-   zero-gradient (clamped) ends.  Problems are packed into bins of up to 4096
+   zero-gradient (clamped) ends.  Problems are packed into bins of up to 6144
    nodes; one persistent kernel launch advances every bin K steps, each CTA
    holding its bin in shared memory, and the launch sequence is captured once
    in a CUDA graph and replayed.  Host arrays are float64 in the caller's

@@ -2,12 +2,13 @@
 // advanced by persistent kernel launches replayed from a CUDA graph.
 //
 // Layout.  At creation the problems are packed (best fit, longest first)
-// into bins of at most BIN_CAP = 4096 nodes and BIN_SEGS problems; the
+// into bins of at most BIN_CAP = 6144 nodes and BIN_SEGS problems; the
 // device state is stored bin after bin, SoA: f[5][Ltot], rho, u, T (float32).
 // Host set/get calls translate to and from the caller's problem order.
 //
 // Kernel.  Each CTA takes bins from a queue, holds one bin in shared memory
-// (populations, rho, u, T, c = sqrt(T): 9 x 16 KB) and advances it K steps
+// (populations, u, T, c = sqrt(T): 8 planes, 196 KB; rho is the sum of the
+// populations) and advances it K steps
 // before taking the next.  A step computes every node of the bin from the
 // shared copy and writes the new level to the bin's global arrays (L2
 // resident); after a barrier the shared copy is restaged.  The per-node step
@@ -47,12 +48,13 @@
 namespace pond {
 namespace batch {
 
-constexpr int BIN_CAP = 4096;
+constexpr int BIN_CAP = 6144;  // nodes per bin (problems are at most MAX_LEN)
+constexpr int MAX_LEN = 4096;
 constexpr int BIN_SEGS = 64;
 constexpr int HARD_MAX = 192;  // parked nodes per bin and step
 constexpr int NPAIR_IN = 21;   // rho, u, T at x-3 .. x+3
 constexpr int NPAIR_OUT = 2;   // converged u, T
-constexpr size_t SMEM = size_t(9) * BIN_CAP * sizeof(float);
+constexpr size_t SMEM = size_t(8) * BIN_CAP * sizeof(float);  // f x5, u, T, c
 
 struct Args {
   float* f;    // [5][Ltot], bin order
@@ -234,13 +236,21 @@ __device__ __forceinline__ void locate(const int* s_seg, int nseg, int x, int& p
   n = s_seg[lo + 1] - ps;
 }
 
+// rho of staged node q: the sum of its populations (the stored rho is that
+// sum after the collision, which conserves it; shared memory holds f, u, T, c)
+__device__ __forceinline__ float rho_of(const float* sf, int q) {
+  float r = sf[q];
+#pragma unroll
+  for (int k = 1; k < 5; k++) r += sf[k * BIN_CAP + q];
+  return r;
+}
+
 // c0.load of bin node x from the shared copy (steps.cu:360-363), with
 // set_base(1, TLat) for an empty record.
-__device__ __forceinline__ void load_node(const float* sf, const float* sr, const float* su, const float* sT, int x,
-                                          Node& s) {
+__device__ __forceinline__ void load_node(const float* sf, const float* su, const float* sT, int x, Node& s) {
 #pragma unroll
   for (int k = 0; k < 5; k++) s.f0[k] = sf[k * BIN_CAP + x];
-  s.rho0 = sr[x]; s.U = su[x]; s.T = sT[x];
+  s.rho0 = rho_of(sf, x); s.U = su[x]; s.T = sT[x];
   if (s.rho0 == 0 && s.U == 0 && s.T == 0) {
     s.rho0 = 1; s.T = Lattice<POND_D1Q5>::TLat;
 #pragma unroll
@@ -253,7 +263,7 @@ __device__ __forceinline__ void load_node(const float* sf, const float* sr, cons
 // BGK toward rho w_i in the co-moving gauge (steps.cu:557-564), the new
 // level to global memory and the node's training pair.
 __device__ __forceinline__ void finish_node(const Args& a, Node& s, long long off, int ps, int n, bool sample,
-                                            const float* sr, const float* su, const float* sT) {
+                                            const float* sf, const float* su, const float* sT) {
   const float rr = float(s.rho0);
   const long long g = off + s.x;
 #pragma unroll
@@ -272,7 +282,7 @@ __device__ __forceinline__ void finish_node(const Args& a, Node& s, long long of
 #pragma unroll
       for (int o = -3; o <= 3; o++) {
         const int q = ps + min(max(xl + o, 0), n - 1);
-        X[o + 3] = sr[q];
+        X[o + 3] = rho_of(sf, q);
         X[7 + o + 3] = su[q];
         X[14 + o + 3] = sT[q];
       }
@@ -288,10 +298,9 @@ __global__ void __launch_bounds__(NT, 1) batch_kernel(Args a) {
   constexpr int GROUP = SCHEME == POND_WENO5 ? 5 : 4;  // lanes per population in phase 2
   extern __shared__ __align__(16) float sm[];
   float* sf = sm;                // [5][BIN_CAP]
-  float* sr = sm + 5 * BIN_CAP;  // rho
-  float* su = sm + 6 * BIN_CAP;  // u
-  float* sT = sm + 7 * BIN_CAP;  // T
-  float* sc = sm + 8 * BIN_CAP;  // c = sqrts(T / TLat)
+  float* su = sm + 5 * BIN_CAP;  // u
+  float* sT = sm + 6 * BIN_CAP;  // T
+  float* sc = sm + 7 * BIN_CAP;  // c = sqrts(T / TLat)
   __shared__ int s_seg[BIN_SEGS + 1];
   __shared__ Node s_hard[HARD_MAX];
   __shared__ int s_bin, s_next, s_nhard, s_hnext;
@@ -314,7 +323,6 @@ __global__ void __launch_bounds__(NT, 1) batch_kernel(Args a) {
       for (int i = tid; i < fill; i += NT) {
 #pragma unroll
         for (int k = 0; k < 5; k++) sf[k * BIN_CAP + i] = finite_or_zero(a.f[k * a.Ltot + off + i]);
-        sr[i] = a.rho[off + i];
         su[i] = a.u[off + i];
         const float T = a.T[off + i];
         sT[i] = T;
@@ -327,7 +335,7 @@ __global__ void __launch_bounds__(NT, 1) batch_kernel(Args a) {
       Node s;
       int ps = 0, n = 1;
       if (tid < fill) {
-        load_node(sf, sr, su, sT, tid, s);
+        load_node(sf, su, sT, tid, s);
         locate(s_seg, nseg, tid, ps, n);
       } else {
         s.x = fill;
@@ -352,11 +360,11 @@ __global__ void __launch_bounds__(NT, 1) batch_kernel(Args a) {
           it_sum += s.niter;
           nc += ok ? 0 : 1;
           it_max = max(it_max, s.niter);
-          finish_node(a, s, off, ps, n, sample, sr, su, sT);
+          finish_node(a, s, off, ps, n, sample, sf, su, sT);
         }
         const int x = atomicAdd(&s_next, 1);
         if (x < fill) {
-          load_node(sf, sr, su, sT, x, s);
+          load_node(sf, su, sT, x, s);
           locate(s_seg, nseg, x, ps, n);
         } else {
           s.x = fill;
@@ -408,7 +416,7 @@ __global__ void __launch_bounds__(NT, 1) batch_kernel(Args a) {
           it_sum += w.niter;
           nc += ok ? 0 : 1;
           it_max = max(it_max, w.niter);
-          finish_node(a, w, off, ps, n, sample, sr, su, sT);
+          finish_node(a, w, off, ps, n, sample, sf, su, sT);
         }
       }
       __syncthreads();  // the new level is in global memory; the shared copy is free
@@ -601,8 +609,8 @@ int pond_batch_create(int nproblems, const int32_t* lengths, int interp, double 
     return set_error(POND_ERR_ARG, "bad tau, max_iter or tolerance");
   long long Ltot = 0;
   for (int p = 0; p < nproblems; p++) {
-    if (lengths[p] < 1 || lengths[p] > batch::BIN_CAP)
-      return set_error(POND_ERR_ARG, "problem %d has length %d (allowed 1..%d)", p, lengths[p], batch::BIN_CAP);
+    if (lengths[p] < 1 || lengths[p] > batch::MAX_LEN)
+      return set_error(POND_ERR_ARG, "problem %d has length %d (allowed 1..%d)", p, lengths[p], batch::MAX_LEN);
     Ltot += lengths[p];
   }
   cudaError_t e = cudaSetDevice(device);

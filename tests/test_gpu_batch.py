@@ -144,7 +144,12 @@ def test_training_pairs(pond):
         b.set_state(rho, u, T)
         b.set_pairs(X, Y, every=2, stride=stride)
         for s in range(4):
-            _, r0, u0, t0 = b.get_state()
+            f0, _, u0, t0 = b.get_state()
+            # rho in a pair is the sum of the node's populations, in float32, in class order
+            r0 = f0[0].astype(np.float32)
+            for k in range(1, 5):
+                r0 = r0 + f0[k].astype(np.float32)
+            r0 = r0.astype(np.float64)
             b.run(1)
             _, r1, u1, t1 = b.get_state()
             if s % 2:
