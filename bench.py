@@ -114,34 +114,18 @@ class ClockSampler:
 
 # ------------------------------------------------------------------ distributed plumbing
 def dist_setup(n_gpus):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    pg = None
-    if world > 1:
-        import datetime
-
-        import torch
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
-        pg = dist
-    return rank, local, world, pg
+    from lbmpond_b200 import replicas
+    return replicas.setup("nccl")
 
 
 def barrier(pg):
-    if pg is not None:
-        pg.barrier()
+    from lbmpond_b200 import replicas
+    replicas.barrier(pg)
 
 
 def allmax(pg, v):
-    if pg is None:
-        return v
-    import torch
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    pg.all_reduce(t, op=pg.ReduceOp.MAX)
-    return float(t.item())
+    from lbmpond_b200 import replicas
+    return replicas.max_over_ranks(pg, v)
 
 
 # ------------------------------------------------------------------ CPU baseline (oracle)
@@ -409,39 +393,51 @@ def run_ours(args, rank, local, world, pg):
     return out
 
 
-def run_batch1d(steps=1000, nproblems=4096):
+def run_batch1d(steps=1000, nproblems=4096, pg=None, rank=0, world=1):
     """The batched D1Q5 workload: `nproblems` seeded Riemann problems
     (lengths uniform in [256, 4096], rho and p log-uniform in [0.1, 10], u
     uniform in [-1, 1], jump at the midpoint), WENO5, tau 0.9, float32 with
     float64 moments, `steps` steps in persistent graph-replayed launches of
-    50 steps after the autotuner picked the tile.  Reported beside the
-    D3Q27 line; problems whose state became non-finite are counted (the
-    float64 oracle diverges on the same strong-jump problems)."""
+    50 steps after the autotuner picked the tile.  Problems whose state
+    became non-finite are counted (the float64 oracle diverges on the same
+    strong-jump problems).  Under several ranks the problems are split by
+    node count (strong scaling: the whole set is the job) and the time is the
+    slowest rank's."""
+    from lbmpond_b200 import replicas
     from lbmpond_b200.batch import Batch, riemann_problems
     import torch
     lengths, rho, u, T = riemann_problems(nproblems, seed=0)
+    off = np.concatenate([[0], np.cumsum(lengths)])
+    mine = replicas.partition_problems(lengths, world)[rank]
+    sel = np.concatenate([np.arange(off[p], off[p + 1]) for p in mine])
+    lengths, rho, u, T = lengths[mine], rho[sel], u[sel], T[sel]
     with Batch(lengths, interp=8, tau=0.9) as b:
         b.set_state(rho, u, T)
         tile, _ = b.autotune(probe_steps=5)
         b.set_state(rho, u, T)
-        ms = b.run(steps, steps_per_launch=50)
+        replicas.barrier(pg)
+        ms = replicas.max_over_ranks(pg, b.run(steps, steps_per_launch=50))
         st = b.stats()
         f, r, uu, tt = b.get_state()
         fin = np.isfinite(f).all(0) & np.isfinite(r) & np.isfinite(uu) & np.isfinite(tt)
-        bad = int(sum(not fin[b.offsets[p]:b.offsets[p + 1]].all() for p in range(nproblems)))
+        bad = int(sum(not fin[b.offsets[p]:b.offsets[p + 1]].all() for p in range(lengths.size)))
         cap = 1 << 21
         X = torch.empty((cap, 21), dtype=torch.float32, device="cuda")
         Y = torch.empty((cap, 2), dtype=torch.float32, device="cuda")
         b.set_state(rho, u, T)
         b.set_pairs(X, Y, every=10, stride=16)
-        ms_pairs = b.run(100, steps_per_launch=50)
+        ms_pairs = replicas.max_over_ranks(pg, b.run(100, steps_per_launch=50))
         pairs = b.pairs_written()
-        nodes = b.nodes
+        nodes = replicas.sum_over_ranks(pg, b.nodes)
+    niter = replicas.sum_over_ranks(pg, st["niter_sum"])
+    nonconv = replicas.sum_over_ranks(pg, st["nonconverged"])
     return {"workload": f"{nproblems} D1Q5 Riemann problems, lengths U[256,4096] (seed 0), WENO5, {steps} steps",
-            "nodes": nodes, "MLUPS": nodes * steps / (ms / 1e3) / 1e6, "ms_per_step": ms / steps,
-            "tile": {"threads": tile[0], "lane_cap": tile[1]}, "niter_mean": st["niter_sum"] / (nodes * steps),
-            "nonconverged_frac": st["nonconverged"] / (nodes * steps), "nonfinite_problems": bad,
-            "pairs": {"rows_per_100_steps": pairs, "every": 10, "stride": 16,
+            "nodes": int(nodes), "MLUPS": nodes * steps / (ms / 1e3) / 1e6, "ms_per_step": ms / steps,
+            "n_gpus": world, "scaling": "strong (problems split across ranks)" if world > 1 else None,
+            "tile": {"threads": tile[0], "lane_cap": tile[1]}, "niter_mean": niter / (nodes * steps),
+            "nonconverged_frac": nonconv / (nodes * steps),
+            "nonfinite_problems": int(replicas.sum_over_ranks(pg, bad)),
+            "pairs": {"rows_per_100_steps": int(replicas.sum_over_ranks(pg, pairs)), "every": 10, "stride": 16,
                       "ms_per_step_with_pairs": ms_pairs / 100}}
 
 
@@ -626,8 +622,13 @@ def main():
         print(json.dumps(run_reference(args, rank, world)), flush=True)
         return
     if args.workload == "batch1d":
-        if int(os.environ.get("RANK", "0")) == 0:
-            print(json.dumps(run_batch1d(args.batch_steps, args.batch_problems)), flush=True)
+        rank, local, world, pg = dist_setup(args.gpus)
+        out = run_batch1d(args.batch_steps, args.batch_problems, pg, rank, world)
+        if pg is not None:
+            pg.barrier()
+            pg.destroy_process_group()
+        if rank == 0:
+            print(json.dumps(out), flush=True)
         return
     if args.workload == "configs":
         if int(os.environ.get("RANK", "0")) == 0:
