@@ -174,3 +174,38 @@ def test_init_and_errors(pond):
         s.init("tgv", 0.05, 0.1, 1.0, 5.0 / 3.0)
         s.step(2)
         assert s.diagnostics()["k"] > 0
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("fault", ["nan_population", "nan_velocity", "negative_T"])
+@pytest.mark.parametrize("lat,shape,interp", [(1, (8, 8, 8), 4), (0, (64, 1, 1), 4), (2, (5, 4, 4), 6)])
+def test_faulty_input_node(orc, pond, lat, shape, interp, fault, precision):
+    """Host-side fault injection: one node of the input carries a NaN
+    population, a NaN velocity or a negative temperature.  The step must
+    give the oracle's result: the same non-finite nodes, and agreement on
+    all the others (the reference drops non-finite transfer terms,
+    steps.cu:390,516,542)."""
+    dim = 1 if lat == 0 else 3
+    rho, g = smooth_state(shape, dim, seed=4, modes=1, du=0.03)
+    f = perturbed_populations(orc, lat, rho, g, seed=4, eps=0.01)
+    if fault == "nan_population":
+        f[3, 10] = np.nan
+    elif fault == "nan_velocity":
+        g[0, 10] = np.nan
+    else:
+        g[3, 10] = -abs(g[3, 10])
+    st = orc.State(f, rho, g)
+    ref, _, _ = orc.step(st, lat, shape, interp=interp, tau=0.8)
+    with pond.Solver(lattice=lat, shape=shape, interp=interp, precision=precision, tau=0.8) as s:
+        s.set_state(rho, g, f=f)
+        s.step(1)
+        fo, ro, go = s.get_state()
+    fin_ref = np.isfinite(ref.f).all(0) & np.isfinite(ref.rho) & np.isfinite(ref.g).all(0)
+    fin_gpu = np.isfinite(fo).all(0) & np.isfinite(ro) & np.isfinite(go).all(0)
+    assert np.array_equal(fin_ref, fin_gpu), (np.flatnonzero(~fin_ref), np.flatnonzero(~fin_gpu))
+    assert fin_ref.sum() >= rho.size - 1
+    tol = TOL[precision]
+    k = fin_ref
+    assert np.abs(ro[k] - ref.rho[k]).max() <= tol * np.abs(ref.rho[k]).max()
+    assert np.abs(go[3][k] - ref.g[3][k]).max() <= tol * np.abs(ref.g[3][k]).max()
+    assert np.abs(fo[:, k] - ref.f[:, k]).max() <= tol * np.abs(ref.f[:, k]).max()
