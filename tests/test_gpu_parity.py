@@ -209,3 +209,33 @@ def test_faulty_input_node(orc, pond, lat, shape, interp, fault, precision):
     assert np.abs(ro[k] - ref.rho[k]).max() <= tol * np.abs(ref.rho[k]).max()
     assert np.abs(go[3][k] - ref.g[3][k]).max() <= tol * np.abs(ref.g[3][k]).max()
     assert np.abs(fo[:, k] - ref.f[:, k]).max() <= tol * np.abs(ref.f[:, k]).max()
+
+
+@pytest.mark.parametrize("precision,l1_tol", [("fp64", 1e-10), ("fp32", 2e-6)])
+def test_twenty_steps_l1_and_drift(orc, pond, precision, l1_tol):
+    """20 steps of a D3Q27 blast (16^3, cubic): L1(rho) and L1(T) against the
+    float64 oracle after the run, and the mass/energy drift of the run equal
+    to the oracle's (the drift is the scheme's: semi-Lagrangian
+    interpolation is not conservative)."""
+    shape, lat, interp, tau = (16, 16, 16), 1, 4, 0.6
+    sphere = (0.5, 0.5, 0.5, 0.3, 1.0, 0.08, 0.3, 0.05)
+    with pond.Solver(lattice="D3Q27", shape=shape, interp=interp, precision=precision, tau=tau) as s:
+        s.init("sphere", *sphere)
+        f0, r0, g0 = s.get_state()
+        d0 = s.diagnostics()
+        s.step(20)
+        f1, r1, g1 = s.get_state()
+        d1 = s.diagnostics()
+    ref = orc.State(f0, r0, g0)
+    e0 = orc.diagnostics(ref, lat, shape)
+    for _ in range(20):
+        ref, _, nc = orc.step(ref, lat, shape, interp=interp, tau=tau)
+        assert nc == 0
+    e1 = orc.diagnostics(ref, lat, shape)
+    l1 = lambda a, b: np.abs(a - b).mean() / np.abs(b).mean()  # noqa: E731
+    assert l1(r1, ref.rho) <= l1_tol and l1(g1[3], ref.g[3]) <= l1_tol
+    dm_gpu = (d1["mass"] - d0["mass"]) / d0["mass"]
+    dm_ref = (e1["mass"] - e0["mass"]) / e0["mass"]
+    de_gpu = (d1["enrg"] - d0["enrg"]) / d0["enrg"]
+    de_ref = (e1["enrg"] - e0["enrg"]) / e0["enrg"]
+    assert abs(dm_gpu - dm_ref) <= 50 * l1_tol and abs(de_gpu - de_ref) <= 50 * l1_tol
