@@ -3,7 +3,8 @@
 //
 // Layout.  At creation the problems are packed (best fit, longest first)
 // into bins of at most BIN_CAP = 6144 nodes and BIN_SEGS problems; the
-// device state is stored bin after bin, SoA: f[5][Ltot], rho, u, T (float32).
+// device state is stored bin after bin, SoA: f[5][S], rho, u, T (float32),
+// every bin starting on a 4-node (16-byte) boundary, S the padded total.
 // Host set/get calls translate to and from the caller's problem order.
 //
 // Kernel.  Each CTA takes bins from a queue, holds one bin in shared memory
@@ -11,7 +12,9 @@
 // populations) and advances it K steps
 // before taking the next.  A step computes every node of the bin from the
 // shared copy and writes the new level to the bin's global arrays (L2
-// resident); after a barrier the shared copy is restaged.  The per-node step
+// resident); after a barrier the shared copy is restaged.  Staging is seven
+// bulk copies (cp.async.bulk, the TMA engine) issued by one thread and
+// completed on an mbarrier whose wait is bounded.  The per-node step
 // is LBMpull (steps.cu:356-588) on D1Q5 with WENO5 (propagateWENO<3,5>,
 // steps.cu:774-825) or cubic Lagrange (propagate<4>, steps.cu:986):
 // float32 populations, transforms and interpolation, float64 moments
@@ -57,12 +60,12 @@ constexpr int NPAIR_OUT = 2;   // converged u, T
 constexpr size_t SMEM = size_t(8) * BIN_CAP * sizeof(float);  // f x5, u, T, c
 
 struct Args {
-  float* f;    // [5][Ltot], bin order
-  float* rho;  // [Ltot]
+  float* f;    // [5][stride], bin order
+  float* rho;  // [stride]
   float* u;
   float* T;
-  long long Ltot;
-  const long long* bin_off;  // [B+1]
+  long long stride;          // plane length: the node count with every bin start padded to 4 nodes
+  const long long* bin_off;  // [B+1] first node of each bin (a multiple of 4)
   const int* seg_first;      // [B+1] into segs
   const int* segs;           // per bin: local problem starts, then the fill
   int B;
@@ -79,6 +82,7 @@ struct Args {
   unsigned long long* pcount;
   long long pcap;
   int pair_every, pair_stride;
+  int* err;  // set when a staging copy did not complete in time
 };
 
 // One node's iteration state.
@@ -269,7 +273,7 @@ __device__ __forceinline__ void finish_node(const Args& a, Node& s, long long of
 #pragma unroll
   for (int k = 0; k < 5; k++) {
     const float fk = s.f0[k] + a.dtau * (rr * float(lattice_weight_t<POND_D1Q5>(k)) - s.f0[k]);
-    a.f[k * a.Ltot + g] = fk;
+    a.f[k * a.stride + g] = fk;
   }
   a.rho[g] = rr;
   a.u[g] = float(s.U);
@@ -292,6 +296,42 @@ __device__ __forceinline__ void finish_node(const Args& a, Node& s, long long of
   }
 }
 
+// ---- bin staging with the bulk-copy (TMA) engine: thread 0 posts the byte
+// count on an mbarrier and issues one cp.async.bulk per plane; every thread
+// waits on the barrier's phase.  Plane segments start 16-byte aligned (bin
+// starts and the plane stride are multiples of 4 nodes).
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_addr(bar)) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+// true once the barrier has completed the phase with this parity (bounded poll)
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+  for (int spin = 0; spin < (1 << 22); spin++) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
 template <int SCHEME, int NT>
 __global__ void __launch_bounds__(NT, 1) batch_kernel(Args a) {
   using L = Lattice<POND_D1Q5>;
@@ -304,7 +344,11 @@ __global__ void __launch_bounds__(NT, 1) batch_kernel(Args a) {
   __shared__ int s_seg[BIN_SEGS + 1];
   __shared__ Node s_hard[HARD_MAX];
   __shared__ int s_bin, s_next, s_nhard, s_hnext;
+  __shared__ __align__(8) unsigned long long s_bar;
   const int tid = threadIdx.x, lane = tid & 31;
+  if (tid == 0) mbar_init(&s_bar);
+  __syncthreads();
+  unsigned phase = 0;
   const int step0 = *a.istep;
   unsigned long long it_sum = 0, nc = 0;
   int it_max = 0;
@@ -314,18 +358,34 @@ __global__ void __launch_bounds__(NT, 1) batch_kernel(Args a) {
     const int bin = s_bin;
     if (bin >= a.B) break;
     const long long off = a.bin_off[bin];
-    const int fill = int(a.bin_off[bin + 1] - off);
     const int sf0 = a.seg_first[bin];
     const int nseg = a.seg_first[bin + 1] - sf0 - 1;
+    const int fill = a.segs[sf0 + nseg];
     for (int i = tid; i <= nseg; i += NT) s_seg[i] = a.segs[sf0 + i];
     for (int step = 0; step < a.nsteps; step++) {
-      // stage the bin's current level (first from HBM, then from L2)
+      // stage the bin's current level (first from HBM, then from L2) by bulk copies
+      if (tid == 0) {  // bins are never empty; fill <= BIN_CAP, a multiple of 4
+        const unsigned bytes = unsigned((fill + 3) & ~3) * sizeof(float);
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // earlier generic use of the buffer
+        mbar_expect(&s_bar, 7 * bytes);
+#pragma unroll
+        for (int k = 0; k < 5; k++) bulk_g2s(sf + k * BIN_CAP, a.f + k * a.stride + off, bytes, &s_bar);
+        bulk_g2s(su, a.u + off, bytes, &s_bar);
+        bulk_g2s(sT, a.T + off, bytes, &s_bar);
+      }
+      const bool staged = mbar_wait(&s_bar, phase & 1u);
+      phase++;
+      if (__syncthreads_or(!staged)) {  // a copy did not land: report, give it one more bounded wait, leave
+        if (tid == 0) {
+          atomicExch(a.err, 1);
+          mbar_wait(&s_bar, (phase - 1) & 1u);
+        }
+        return;
+      }
       for (int i = tid; i < fill; i += NT) {
 #pragma unroll
-        for (int k = 0; k < 5; k++) sf[k * BIN_CAP + i] = finite_or_zero(a.f[k * a.Ltot + off + i]);
-        su[i] = a.u[off + i];
-        const float T = a.T[off + i];
-        sT[i] = T;
+        for (int k = 0; k < 5; k++) sf[k * BIN_CAP + i] = finite_or_zero(sf[k * BIN_CAP + i]);
+        const float T = sT[i];
         sc[i] = copysignf(sqrtf(fabsf(T) * float(1.0 / L::TLat)), T);
       }
       if (tid == 0) { s_next = NT; s_nhard = 0; s_hnext = 0; }
@@ -419,6 +479,8 @@ __global__ void __launch_bounds__(NT, 1) batch_kernel(Args a) {
           finish_node(a, w, off, ps, n, sample, sf, su, sT);
         }
       }
+      // this thread's global writes of the new level, before the next bulk copy reads them
+      asm volatile("fence.proxy.async.global;\n" ::: "memory");
       __syncthreads();  // the new level is in global memory; the shared copy is free
     }
   }
@@ -444,7 +506,8 @@ struct pond_batch {
   int device = 0;
   int P = 0;
   int B = 0;
-  long long Ltot = 0;
+  long long Ltot = 0;    // nodes of all problems
+  long long stride = 0;  // device plane length: bins start on 4-node (16-byte) boundaries
   int interp = POND_WENO5;
   double tau = 0.9, tol_abs = 1e-7, tol_rel = 1e-6;
   int max_iter = 100;
@@ -463,6 +526,7 @@ struct pond_batch {
   int* istep_dev = nullptr;
   unsigned long long* stats = nullptr;
   unsigned long long* pcount = nullptr;
+  int* err = nullptr;
   float* px = nullptr;
   float* py = nullptr;
   long long pcap = 0;
@@ -498,7 +562,7 @@ static void* kernel_for(int interp, int threads) {
 // Enqueue one K-step chunk: queue reset, the persistent kernel, step counter.
 static int enqueue_chunk(pond_batch* b, int k, cudaStream_t s) {
   Args a;
-  a.f = b->f; a.rho = b->rho; a.u = b->u; a.T = b->T; a.Ltot = b->Ltot;
+  a.f = b->f; a.rho = b->rho; a.u = b->u; a.T = b->T; a.stride = b->stride;
   a.bin_off = b->bin_off; a.seg_first = b->seg_first; a.segs = b->segs; a.B = b->B;
   a.queue = b->queue; a.istep = b->istep_dev; a.nsteps = k;
   a.dtau = float(1.0 / b->tau); a.tol_abs = b->tol_abs; a.tol_rel = b->tol_rel; a.max_iter = b->max_iter;
@@ -506,6 +570,7 @@ static int enqueue_chunk(pond_batch* b, int k, cudaStream_t s) {
   a.stats = b->stats;
   a.px = b->pair_every > 0 ? b->px : nullptr; a.py = b->py; a.pcount = b->pcount; a.pcap = b->pcap;
   a.pair_every = b->pair_every > 0 ? b->pair_every : 1; a.pair_stride = b->pair_stride;
+  a.err = b->err;
   void* kern = kernel_for(b->interp, b->threads);
   cudaError_t e = cudaMemsetAsync(b->queue, 0, sizeof(int), s);
   if (e != cudaSuccess) return cuda_fail(e, "batch queue reset");
@@ -590,7 +655,7 @@ int pond_batch_destroy(pond_batch* b) {
   batch::drop_graph(b);
   cudaFree(b->f); cudaFree(b->rho); cudaFree(b->u); cudaFree(b->T);
   cudaFree(b->bin_off); cudaFree(b->seg_first); cudaFree(b->segs);
-  cudaFree(b->queue); cudaFree(b->istep_dev); cudaFree(b->stats); cudaFree(b->pcount);
+  cudaFree(b->queue); cudaFree(b->istep_dev); cudaFree(b->stats); cudaFree(b->pcount); cudaFree(b->err);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
   if (b->stream) cudaStreamDestroy(b->stream);
@@ -633,22 +698,25 @@ int pond_batch_create(int nproblems, const int32_t* lengths, int interp, double 
       local += lengths[p];
     }
     segs.push_back(local);
-    bin_off[bi + 1] = bin_off[bi] + local;
+    bin_off[bi + 1] = (bin_off[bi] + local + 3) & ~3LL;  // bulk copies start 16-byte aligned
   }
   seg_first[b->B] = (int)segs.size();
+  const long long S = bin_off[b->B];
+  b->stride = S;
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
   b->grid = std::min(b->B, nsm);  // one resident CTA per SM (a bin fills most of shared memory)
-  bool ok = cudaMalloc(&b->f, 5 * Ltot * sizeof(float)) == cudaSuccess &&
-            cudaMalloc(&b->rho, Ltot * sizeof(float)) == cudaSuccess &&
-            cudaMalloc(&b->u, Ltot * sizeof(float)) == cudaSuccess &&
-            cudaMalloc(&b->T, Ltot * sizeof(float)) == cudaSuccess &&
+  bool ok = cudaMalloc(&b->f, 5 * S * sizeof(float)) == cudaSuccess &&
+            cudaMalloc(&b->rho, S * sizeof(float)) == cudaSuccess &&
+            cudaMalloc(&b->u, S * sizeof(float)) == cudaSuccess &&
+            cudaMalloc(&b->T, S * sizeof(float)) == cudaSuccess &&
             cudaMalloc(&b->bin_off, bin_off.size() * sizeof(long long)) == cudaSuccess &&
             cudaMalloc(&b->seg_first, seg_first.size() * sizeof(int)) == cudaSuccess &&
             cudaMalloc(&b->segs, segs.size() * sizeof(int)) == cudaSuccess &&
             cudaMalloc(&b->queue, sizeof(int)) == cudaSuccess && cudaMalloc(&b->istep_dev, sizeof(int)) == cudaSuccess &&
             cudaMalloc(&b->stats, 3 * sizeof(unsigned long long)) == cudaSuccess &&
             cudaMalloc(&b->pcount, sizeof(unsigned long long)) == cudaSuccess &&
+            cudaMalloc(&b->err, sizeof(int)) == cudaSuccess &&
             cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess &&
             cudaEventCreate(&b->ev0) == cudaSuccess && cudaEventCreate(&b->ev1) == cudaSuccess;
   if (!ok) {
@@ -663,6 +731,12 @@ int pond_batch_create(int nproblems, const int32_t* lengths, int interp, double 
   if (e == cudaSuccess) e = cudaMemset(b->istep_dev, 0, sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(b->pcount, 0, sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaMemset(b->stats, 0, 3 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMemset(b->err, 0, sizeof(int));
+  // padding nodes between bins are copied along with the bins but never read
+  if (e == cudaSuccess) e = cudaMemset(b->f, 0, 5 * S * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemset(b->rho, 0, S * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemset(b->u, 0, S * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemset(b->T, 0, S * sizeof(float));
   for (int t : {256, 512, 768, 1024})
     for (int s : {POND_WENO5, POND_LAGR4})
       if (e == cudaSuccess)
@@ -681,7 +755,7 @@ int32_t pond_batch_bins(const pond_batch* b) { return b ? b->B : 0; }
 
 int pond_batch_set_state(pond_batch* b, const double* rho, const double* u, const double* T) {
   if (!b || !rho || !u || !T) return set_error(POND_ERR_ARG, "pond_batch_set_state: null argument");
-  const long long n = b->Ltot;
+  const long long n = b->stride;
   std::vector<float> fb(5 * n), rb(n), ub(n), tb(n);
   long long src = 0;
   for (int p = 0; p < b->P; p++) {
@@ -710,7 +784,7 @@ int pond_batch_get_state(pond_batch* b, double* f, double* rho, double* u, doubl
   cudaSetDevice(b->device);
   cudaError_t e = cudaStreamSynchronize(b->stream);
   if (e != cudaSuccess) return cuda_fail(e, "pond_batch_get_state");
-  const long long n = b->Ltot;
+  const long long n = b->stride, nu = b->Ltot;
   std::vector<float> tmp(5 * n);
   struct Item {
     double* dst;
@@ -722,7 +796,7 @@ int pond_batch_get_state(pond_batch* b, double* f, double* rho, double* u, doubl
     e = cudaMemcpy(tmp.data(), it.src, it.comps * n * sizeof(float), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_fail(e, "pond_batch_get_state");
     for (int k = 0; k < it.comps; k++) {
-      long long dst = (long long)k * n;
+      long long dst = (long long)k * nu;
       for (int p = 0; p < b->P; p++) {
         const float* s = tmp.data() + (long long)k * n + b->pos[p];
         for (int i = 0; i < b->len[p]; i++) it.dst[dst++] = s[i];
@@ -774,6 +848,13 @@ int pond_batch_run(pond_batch* b, int nsteps, int k, float* ms) {
   e = cudaEventRecord(b->ev1, b->stream);
   if (e == cudaSuccess) e = cudaEventSynchronize(b->ev1);
   if (e != cudaSuccess) return cuda_fail(e, "pond_batch_run");
+  int err = 0;
+  e = cudaMemcpy(&err, b->err, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(e, "pond_batch_run");
+  if (err) {
+    cudaMemset(b->err, 0, sizeof(int));
+    return set_error(POND_ERR_CUDA, "pond_batch_run: a bin staging copy did not complete; the state is undefined");
+  }
   float t = 0;
   cudaEventElapsedTime(&t, b->ev0, b->ev1);
   if (ms) *ms = t;
@@ -819,7 +900,7 @@ int pond_batch_autotune(pond_batch* b, int probe_steps, const int32_t* tiles, in
       return set_error(POND_ERR_ARG, "autotune candidate %d is not a valid tile", c);
   }
   cudaSetDevice(b->device);
-  const long long n = b->Ltot;
+  const long long n = b->stride;
   float* snap = nullptr;
   int istep_dev = 0;
   cudaError_t e = cudaMalloc(&snap, 8 * n * sizeof(float));
