@@ -149,9 +149,11 @@ int pond_download_state(pond_ctx* ctx, void* f, void* rho, void* g);
 /* copy the state of src into dst (same lattice and grid; the precision is
    converted on the device): both stored time levels and the step counter */
 int pond_copy_state(pond_ctx* dst, pond_ctx* src);
-/* stencil nodes transformed during the last step, summed over nodes and
-   iterations (the work count behind the compute roofline) */
-int pond_last_step_work(pond_ctx* ctx, int64_t* transformed_nodes);
+/* work of the last step, summed over nodes and iterations (the count behind
+   the compute roofline): for the D3Q27 float32 kernel the floating-point
+   operations of its basis contractions (a multiply-add counts 2), for the
+   other kernels the stencil nodes transformed */
+int pond_last_step_work(pond_ctx* ctx, int64_t* work);
 
 /* ---- learned starting gauge ------------------------------------------
    A small network (39 -> H -> H -> 4, tanh, H = 64 or 128; BF16 tensor-core

@@ -9,13 +9,19 @@
 //    u_x, u_y, u_z and c = sqrts(T/TLat), 214 KB) once per step.  Boundary
 //    resolution (periodic wrap, clamp, mirror with population reversal), the
 //    reference's dropping of non-finite terms and the square root of T are
-//    applied while staging, so the iteration loop reads plain SoA planes;
+//    applied while staging;
+//  * after staging, each staged node's 27 populations are replaced by its 27
+//    velocity moments V[k] = sum_b v_b^k f_b (k = 0..2 per axis) in a
+//    velocity frame shared by the CTA.  The transfer of a source node into
+//    the target gauge, sum_b prod_ax L_i(y_b) f_b with y = (v_b - U)/C and
+//    L_i the quadratic Lagrange basis over the target classes, is then
+//    sum_k G[i][k] V[k], where G depends on the target gauge only; so the
+//    interpolation weights and G are contracted against the moments one axis
+//    at a time (z per stencil node, y per stencil column, x per stencil row:
+//    81 FMA each) instead of transforming every stencil node (243 FMA);
 //  * the fixed-point iteration is warp-synchronous: a warp iterates while any
 //    of its lanes is unconverged, and walks the stencil offsets common to its
 //    lanes, so a warp's shared-memory loads hit 32 consecutive addresses;
-//  * per stencil node the gauge transform is three 1D passes of the 3x3
-//    Lagrange-basis matrix with the interpolation weights folded into the
-//    rows (243 FMA), accumulated straight into the 27 populations;
 //  * a lane whose departure points leave the +-2 halo (|u| + sqrt(T/TLat) >= 1
 //    along an axis) runs that iteration from global memory instead.
 #pragma once
@@ -47,95 +53,107 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // class index -> its mirror image along one axis (0 <-> 0, + <-> -)
 __device__ __forceinline__ int rev3(int c) { return c == 0 ? 0 : 3 - c; }
 
-// Weighted basis rows of one axis: M[i][b] = w_i * L_i(s + r*xi_b) for the
-// three classes i of the target gauge, xi = {0, +1, -1}.
-__device__ __forceinline__ void weighted_rows(float s, float r, const float w[3], float M[3][3]) {
-  const float y[3] = {s, s + r, s - r};
-  const float hw1 = 0.5f * w[1], hw2 = 0.5f * w[2];
+// Velocity moments of one node along the three axes, in place over its 27
+// populations (tensor-class order, xi = {0, +1, -1} per axis):
+//   V[k1,k2,k3] = sum_b vx_b^k1 vy_b^k2 vz_b^k3 f_b,  v_b = d + c_ax xi_b,
+// with d = u - u_ref (a velocity frame shared by the CTA) and c_ax the
+// node's sqrts(T/TLat) (negated on a mirrored axis, which reverses the
+// classes along it).  Per axis: S = f+ + f-, D = f+ - f-,
+//   V0 = f0 + S,  V1 = d V0 + c D,  V2 = d V1 + c (d D + c S).
+__device__ __forceinline__ void node_moments(float v[27], const float d[3], const float c[3]) {
 #pragma unroll
-  for (int b = 0; b < 3; b++) {
-    const float t = w[0] * y[b];
-    M[0][b] = fmaf(-t, y[b], w[0]);      // w0 (1 - y^2)
-    const float u = hw1 * y[b];
-    M[1][b] = fmaf(u, y[b], u);          // w1 y (y + 1) / 2
-    const float v = hw2 * y[b];
-    M[2][b] = fmaf(v, y[b], -v);         // w2 y (y - 1) / 2
-  }
-}
-
-// acc[ix,iy,iz] += sum_j Mx[ix][jx] My[iy][jy] Mz[iz][jz] f[jx,jy,jz]
-__device__ __forceinline__ void transform_accumulate(const float fn[27], const float Mx[3][3], const float My[3][3],
-                                                     const float Mz[3][3], float acc[27]) {
-  float t1[3][3][3];
+  for (int ax = 0; ax < 3; ax++) {
+    const int st = ax == 0 ? 9 : ax == 1 ? 3 : 1;
 #pragma unroll
-  for (int jx = 0; jx < 3; jx++)
-#pragma unroll
-    for (int jy = 0; jy < 3; jy++)
-#pragma unroll
-      for (int iz = 0; iz < 3; iz++)
-        t1[jx][jy][iz] = fmaf(Mz[iz][2], fn[jx * 9 + jy * 3 + 2],
-                              fmaf(Mz[iz][1], fn[jx * 9 + jy * 3 + 1], Mz[iz][0] * fn[jx * 9 + jy * 3]));
-  float t2[3][3][3];
-#pragma unroll
-  for (int jx = 0; jx < 3; jx++)
-#pragma unroll
-    for (int iy = 0; iy < 3; iy++)
-#pragma unroll
-      for (int iz = 0; iz < 3; iz++)
-        t2[jx][iy][iz] = fmaf(My[iy][2], t1[jx][2][iz], fmaf(My[iy][1], t1[jx][1][iz], My[iy][0] * t1[jx][0][iz]));
-#pragma unroll
-  for (int ix = 0; ix < 3; ix++)
-#pragma unroll
-    for (int iy = 0; iy < 3; iy++)
-#pragma unroll
-      for (int iz = 0; iz < 3; iz++) {
-        float& o = acc[ix * 9 + iy * 3 + iz];
-        o = fmaf(Mx[ix][2], t2[2][iy][iz], fmaf(Mx[ix][1], t2[1][iy][iz], fmaf(Mx[ix][0], t2[0][iy][iz], o)));
-      }
-}
-
-// As transform_accumulate, restricted to the target classes each axis needs
-// at this stencil node (nx/ny/nz: warp-uniform, a class is skipped when its
-// interpolation weight is zero for every lane of the warp).
-__device__ __forceinline__ void transform_accumulate_sel(const float fn[27], const float Mx[3][3],
-                                                         const float My[3][3], const float Mz[3][3],
-                                                         const bool nx[3], const bool ny[3], const bool nz[3],
-                                                         float acc[27]) {
-  float t1[3][3][3];
-#pragma unroll
-  for (int iz = 0; iz < 3; iz++) {
-    if (!nz[iz]) continue;
-#pragma unroll
-    for (int jx = 0; jx < 3; jx++)
-#pragma unroll
-      for (int jy = 0; jy < 3; jy++)
-        t1[jx][jy][iz] = fmaf(Mz[iz][2], fn[jx * 9 + jy * 3 + 2],
-                              fmaf(Mz[iz][1], fn[jx * 9 + jy * 3 + 1], Mz[iz][0] * fn[jx * 9 + jy * 3]));
-  }
-  float t2[3][3][3];
-#pragma unroll
-  for (int iy = 0; iy < 3; iy++) {
-    if (!ny[iy]) continue;
-#pragma unroll
-    for (int iz = 0; iz < 3; iz++) {
-      if (!nz[iz]) continue;
-#pragma unroll
-      for (int jx = 0; jx < 3; jx++)
-        t2[jx][iy][iz] = fmaf(My[iy][2], t1[jx][2][iz], fmaf(My[iy][1], t1[jx][1][iz], My[iy][0] * t1[jx][0][iz]));
+    for (int o = 0; o < 9; o++) {
+      // the two other axes' indices
+      const int base = ax == 0 ? o : ax == 1 ? (o / 3) * 9 + (o % 3) : o * 3;
+      const float f0 = v[base], fp = v[base + st], fm = v[base + 2 * st];
+      const float S = fp + fm, D = fp - fm;
+      const float V0 = f0 + S;
+      const float V1 = fmaf(d[ax], V0, c[ax] * D);
+      const float V2 = fmaf(d[ax], V1, c[ax] * fmaf(d[ax], D, c[ax] * S));
+      v[base] = V0; v[base + st] = V1; v[base + 2 * st] = V2;
     }
   }
+}
+
+// Basis coefficients of one axis for a target gauge (U, C): the Lagrange
+// basis polynomials over the target classes, L_0 = 1 - y^2,
+// L_+ = y (y + 1) / 2, L_- = y (y - 1) / 2, at y = (v - (U - u_ref)) / C
+// = a v + b, expanded in powers of v: L_i(y) = sum_k G[i][k] v^k.
+__device__ __forceinline__ void basis_coeffs(float a, float b, float G[3][3]) {
+  const float a2 = a * a;
+  G[0][0] = fmaf(-b, b, 1.f);
+  G[0][1] = -2.f * a * b;
+  G[0][2] = -a2;
+  G[1][0] = 0.5f * fmaf(b, b, b);
+  G[1][1] = a * (b + 0.5f);
+  G[1][2] = 0.5f * a2;
+  G[2][0] = 0.5f * fmaf(b, b, -b);
+  G[2][1] = a * (b - 0.5f);
+  G[2][2] = 0.5f * a2;
+}
+
+// Z[k1,k2,i3] += sum_k3 w_i3 Gz[i3][k3] V[k1,k2,k3] for the z-classes i3
+// flagged in nz (the first contraction, one per stencil node).
+template <typename LoadV>
+__device__ __forceinline__ void contract_z(const float Gz[3][3], const float wz[3], const bool nz[3], LoadV loadv,
+                                           float Z[27]) {
+  float g[3][3];
 #pragma unroll
-  for (int ix = 0; ix < 3; ix++) {
-    if (!nx[ix]) continue;
+  for (int i = 0; i < 3; i++)
 #pragma unroll
-    for (int iy = 0; iy < 3; iy++) {
-      if (!ny[iy]) continue;
+    for (int k = 0; k < 3; k++) g[i][k] = wz[i] * Gz[i][k];
 #pragma unroll
-      for (int iz = 0; iz < 3; iz++) {
-        if (!nz[iz]) continue;
-        float& o = acc[ix * 9 + iy * 3 + iz];
-        o = fmaf(Mx[ix][2], t2[2][iy][iz], fmaf(Mx[ix][1], t2[1][iy][iz], fmaf(Mx[ix][0], t2[0][iy][iz], o)));
+  for (int k12 = 0; k12 < 9; k12++) {
+    const float v0 = loadv(k12 * 3 + 0), v1 = loadv(k12 * 3 + 1), v2 = loadv(k12 * 3 + 2);
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      if (!nz[i]) continue;
+      float& o = Z[k12 * 3 + i];
+      o = fmaf(g[i][2], v2, fmaf(g[i][1], v1, fmaf(g[i][0], v0, o)));
+    }
+  }
+}
+
+// Y[k1,i2,i3] += sum_k2 w_i2 Gy[i2][k2] Z[k1,k2,i3] (one per stencil column)
+__device__ __forceinline__ void contract_y(const float Gy[3][3], const float wy[3], const bool ny[3], const float Z[27],
+                                           float Y[27]) {
+  float g[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int k = 0; k < 3; k++) g[i][k] = wy[i] * Gy[i][k];
+#pragma unroll
+  for (int k1 = 0; k1 < 3; k1++)
+#pragma unroll
+    for (int i2 = 0; i2 < 3; i2++) {
+      if (!ny[i2]) continue;
+#pragma unroll
+      for (int i3 = 0; i3 < 3; i3++) {
+        float& o = Y[(k1 * 3 + i2) * 3 + i3];
+        o = fmaf(g[i2][2], Z[(k1 * 3 + 2) * 3 + i3],
+                 fmaf(g[i2][1], Z[(k1 * 3 + 1) * 3 + i3], fmaf(g[i2][0], Z[k1 * 9 + i3], o)));
       }
+    }
+}
+
+// acc[i1,i2,i3] += sum_k1 w_i1 Gx[i1][k1] Y[k1,i2,i3] (one per stencil row)
+__device__ __forceinline__ void contract_x(const float Gx[3][3], const float wx[3], const bool nx[3], const float Y[27],
+                                           float acc[27]) {
+  float g[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int k = 0; k < 3; k++) g[i][k] = wx[i] * Gx[i][k];
+#pragma unroll
+  for (int i1 = 0; i1 < 3; i1++) {
+    if (!nx[i1]) continue;
+#pragma unroll
+    for (int i23 = 0; i23 < 9; i23++) {
+      float& o = acc[i1 * 9 + i23];
+      o = fmaf(g[i1][2], Y[18 + i23], fmaf(g[i1][1], Y[9 + i23], fmaf(g[i1][0], Y[i23], o)));
     }
   }
 }
@@ -251,11 +269,29 @@ __global__ void __launch_bounds__(THREADS, 1) pull_d3q27_tile_kernel(StepArgs<fl
     flags[i] = (unsigned char)(fl | (ok ? 0 : 8));
   }
   __syncthreads();
-  // 4) populations post-pass: non-finite values and invalid nodes -> 0
-  for (int idx = tid; idx < 27 * SN; idx += THREADS) {
-    const int i = idx % SN;
-    const float v = sm[idx];
-    sm[idx] = (!(flags[i] & 8) && fabsf(v) <= 3.402823466e38f) ? v : 0.f;
+  // 4) velocity frame of the CTA: the gauge of the tile's centre node
+  float uref[3];
+  {
+    constexpr int ci = (H + TZ / 2) * SX * SY + (H + TY / 2) * SX + (H + TX / 2);
+#pragma unroll
+    for (int k = 0; k < 3; k++) uref[k] = sm[(27 + k) * SN + ci];
+  }
+  // 5) populations -> velocity moments in that frame, in place (non-finite
+  //    populations and every population of an invalid node count as 0)
+  for (int i = tid; i < SN; i += THREADS) {
+    const bool bad = flags[i] & 8;
+    float v[27];
+#pragma unroll
+    for (int t = 0; t < 27; t++) {
+      const float x = sm[t * SN + i];
+      v[t] = (!bad && fabsf(x) <= 3.402823466e38f) ? x : 0.f;
+    }
+    const float c = sm[30 * SN + i];
+    const float d[3] = {sm[27 * SN + i] - uref[0], sm[28 * SN + i] - uref[1], sm[29 * SN + i] - uref[2]};
+    const float cc[3] = {c, c, c};
+    node_moments(v, d, cc);
+#pragma unroll
+    for (int t = 0; t < 27; t++) sm[t * SN + i] = v[t];
   }
   __syncthreads();
 
@@ -264,12 +300,21 @@ __global__ void __launch_bounds__(THREADS, 1) pull_d3q27_tile_kernel(StepArgs<fl
   const bool active = x < a.nx && y < a.ny && z < a.nz;
   NodeSums ns = {0, 0, 0, 0, 0, 0, 0ull, 0ull, 0ull, 0};
   const long long idx = active ? x + (long long)a.nx * (y + (long long)a.ny * z) : 0;
-  float f0[27];
+  // the node's current populations live in shared memory between iterations
+  // (the gauge planes are free once the moments are formed: 4 SN floats =
+  // 27 THREADS floats), which keeps them out of the loop's registers
+  static_assert(4 * SN == 27 * THREADS, "population store must fit the gauge planes");
+  float* f0s = sm + 27 * SN + tid;
   double rho0 = 1, U[3] = {0, 0, 0}, T = L::TLat;
-  if (active) load_center<POND_D3Q27, float>(a, idx, f0, rho0, U, T);
-  else
+  {
+    float f0[27];
+    if (active) load_center<POND_D3Q27, float>(a, idx, f0, rho0, U, T);
+    else
 #pragma unroll
-    for (int t = 0; t < 27; t++) f0[t] = 0.f;
+      for (int t = 0; t < 27; t++) f0[t] = 0.f;
+#pragma unroll
+    for (int t = 0; t < 27; t++) f0s[t * THREADS] = f0[t];
+  }
   const int pos[3] = {x, y, z};
   const int sbase = (lz + H) * SX * SY + (ly + H) * SX + (lx + H);
   bool done = !active;
@@ -296,8 +341,13 @@ __global__ void __launch_bounds__(THREADS, 1) pull_d3q27_tile_kernel(StepArgs<fl
       lo[ax] = min(ro[ax][0], min(ro[ax][1], ro[ax][2]));
       hi[ax] = max(ro[ax][0], max(ro[ax][1], ro[ax][2])) + N - 1;
     }
-    const float invC = __frcp_rn(float(C));
-    const float Us[3] = {float(U[0]) * invC, float(U[1]) * invC, float(U[2]) * invC};
+    // basis coefficients per axis: y = (v + u_ref - U) / C = a v + b
+    const float ainv = __frcp_rn(float(C));
+    float bq[3];
+#pragma unroll
+    for (int ax = 0; ax < 3; ax++) bq[ax] = float((double(uref[ax]) - U[ax]) / C);
+    float Gz[3][3];  // the z basis is used per stencil node; x and y are rebuilt per row and column
+    basis_coeffs(ainv, bq[2], Gz);
     float acc[27];
 #pragma unroll
     for (int t = 0; t < 27; t++) acc[t] = 0.f;
@@ -310,23 +360,44 @@ __global__ void __launch_bounds__(THREADS, 1) pull_d3q27_tile_kernel(StepArgs<fl
         wl[ax] = __reduce_min_sync(0xffffffffu, done ? H : lo[ax]);
         wh[ax] = __reduce_max_sync(0xffffffffu, done ? -H : hi[ax]);
       }
-      if (!done) work += (unsigned long long)(wh[0] - wl[0] + 1) * (wh[1] - wl[1] + 1) * (wh[2] - wl[2] + 1);
+      // per axis, offset and target class: does any unconverged lane of the
+      // warp weight it (bit 3 (o + H) + class); classes nobody weights are skipped
+      unsigned need[3] = {0u, 0u, 0u};
+#pragma unroll
+      for (int ax = 0; ax < 3; ax++)
+#pragma unroll
+        for (int o = -H; o <= H; o++)
+#pragma unroll
+          for (int c = 0; c < 3; c++)
+            if (__any_sync(0xffffffffu, !done && wpick<N>(wt[ax][c], ro[ax][c], o) != 0.f))
+              need[ax] |= 1u << (3 * (o + H) + c);
+      if (!done) {  // floating-point operations of the contractions below
+        const unsigned long long ex = wh[0] - wl[0] + 1, ey = wh[1] - wl[1] + 1, ez = wh[2] - wl[2] + 1;
+        work += ex * ey * (54ull * __popc(need[2]) + 9 * ez) + ex * (54ull * __popc(need[1]) + 9 * ey) +
+                54ull * __popc(need[0]) + 9 * ex;
+      }
       for (int ox = wl[0]; ox <= wh[0]; ox++) {
         float wx[3];
         bool nx[3];
 #pragma unroll
         for (int c = 0; c < 3; c++) {
           wx[c] = wpick<N>(wt[0][c], ro[0][c], ox);
-          nx[c] = __any_sync(0xffffffffu, !done && wx[c] != 0.f);
+          nx[c] = (need[0] >> (3 * (ox + H) + c)) & 1u;
         }
+        float Yr[27];
+#pragma unroll
+        for (int t = 0; t < 27; t++) Yr[t] = 0.f;
         for (int oy = wl[1]; oy <= wh[1]; oy++) {
           float wy[3];
           bool ny[3];
 #pragma unroll
           for (int c = 0; c < 3; c++) {
             wy[c] = wpick<N>(wt[1][c], ro[1][c], oy);
-            ny[c] = __any_sync(0xffffffffu, !done && wy[c] != 0.f);
+            ny[c] = (need[1] >> (3 * (oy + H) + c)) & 1u;
           }
+          float Zc[27];
+#pragma unroll
+          for (int t = 0; t < 27; t++) Zc[t] = 0.f;
 #pragma unroll
           for (int oz = -H; oz <= H; oz++) {
             if (oz < wl[2] || oz > wh[2]) continue;
@@ -335,56 +406,73 @@ __global__ void __launch_bounds__(THREADS, 1) pull_d3q27_tile_kernel(StepArgs<fl
 #pragma unroll
             for (int c = 0; c < 3; c++) {
               wz[c] = wpick<N>(wt[2][c], ro[2][c], oz);
-              nz[c] = __any_sync(0xffffffffu, !done && wz[c] != 0.f);
+              nz[c] = (need[2] >> (3 * (oz + H) + c)) & 1u;
             }
-            const int si = sbase + oz * SX * SY + oy * SX + ox;
-            float fn[27];
-#pragma unroll
-            for (int t = 0; t < 27; t++) fn[t] = sm[t * SN + si];
-            const float cn = sm[30 * SN + si];
-            const float r = cn * invC;
-            float Mx[3][3], My[3][3], Mz[3][3];
-            weighted_rows(fmaf(sm[27 * SN + si], invC, -Us[0]), r, wx, Mx);
-            weighted_rows(fmaf(sm[28 * SN + si], invC, -Us[1]), r, wy, My);
-            weighted_rows(fmaf(sm[29 * SN + si], invC, -Us[2]), r, wz, Mz);
-            transform_accumulate_sel(fn, Mx, My, Mz, nx, ny, nz, acc);
+            const float* sv = sm + (sbase + oz * SX * SY + oy * SX + ox);
+            contract_z(Gz, wz, nz, [&](int t) { return sv[t * SN]; }, Zc);
           }
+          float Gy[3][3];
+          basis_coeffs(ainv, bq[1], Gy);
+          contract_y(Gy, wy, ny, Zc, Yr);
         }
+        float Gx[3][3];
+        basis_coeffs(ainv, bq[0], Gx);
+        contract_x(Gx, wx, nx, Yr, acc);
       }
     } else if (!done) {
       // departure points beyond the staged halo: this lane reads global memory
-      if (!done) work += (unsigned long long)(hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
+      // and forms each stencil node's moments itself
+      const unsigned long long ex = hi[0] - lo[0] + 1, ey = hi[1] - lo[1] + 1, ez = hi[2] - lo[2] + 1;
+      work += ex * ey * ez * 171 + ex * ey * 171 + ex * 171;
+      const bool all3[3] = {true, true, true};
       for (int ox = lo[0]; ox <= hi[0]; ox++) {
         bool rv[3] = {false, false, false};
         const int gx = resolve_axis(x + ox, a.nx, a.bc[0], rv[0]);
         float wx[3];
 #pragma unroll
         for (int c = 0; c < 3; c++) wx[c] = wpick<N>(wt[0][c], ro[0][c], ox);
+        float Yr[27];
+#pragma unroll
+        for (int t = 0; t < 27; t++) Yr[t] = 0.f;
         for (int oy = lo[1]; oy <= hi[1]; oy++) {
           const int gy = resolve_axis(y + oy, a.ny, a.bc[1], rv[1]);
           float wy[3];
 #pragma unroll
           for (int c = 0; c < 3; c++) wy[c] = wpick<N>(wt[1][c], ro[1][c], oy);
+          float Zc[27];
+#pragma unroll
+          for (int t = 0; t < 27; t++) Zc[t] = 0.f;
           for (int oz = lo[2]; oz <= hi[2]; oz++) {
             const int gz = resolve_axis(z + oz, a.nz, a.bc[2], rv[2]);
             float wz[3];
 #pragma unroll
             for (int c = 0; c < 3; c++) wz[c] = wpick<N>(wt[2][c], ro[2][c], oz);
             const long long g = gx + (long long)a.nx * (gy + (long long)a.ny * gz);
-            float fn[27], s[3], r[3];
-            const float Uc[3] = {float(U[0]), float(U[1]), float(U[2])};
-            load_node<POND_D3Q27, float>(a, g, rv, Uc, invC, fn, s, r);
+            const float un[3] = {a.g_in[g], a.g_in[a.N + g], a.g_in[2 * a.N + g]};
             const float Tn = a.g_in[3 * a.N + g];
-            const float un0 = a.g_in[g], un1 = a.g_in[a.N + g], un2 = a.g_in[2 * a.N + g];
-            const bool ok = fabsf(un0) <= 3.0e38f && fabsf(un1) <= 3.0e38f && fabsf(un2) <= 3.0e38f &&
+            const bool ok = fabsf(un[0]) <= 3.0e38f && fabsf(un[1]) <= 3.0e38f && fabsf(un[2]) <= 3.0e38f &&
                             fabsf(Tn) <= 3.0e38f;
-            float Mx[3][3], My[3][3], Mz[3][3];
-            weighted_rows(s[0], r[0], wx, Mx);
-            weighted_rows(s[1], r[1], wy, My);
-            weighted_rows(s[2], r[2], wz, Mz);
-            if (ok) transform_accumulate(fn, Mx, My, Mz, acc);
+            const float cn = copysignf(sqrtf(fabsf(Tn) * (float)(1.0 / L::TLat)), Tn);
+            float v[27];
+#pragma unroll
+            for (int t = 0; t < 27; t++)
+              v[t] = ok ? finite_or_zero_f(__ldg(&a.f_in[(long long)c_ref27[t] * a.N + g])) : 0.f;
+            float d[3], cc[3];
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+              d[k] = ok ? (rv[k] ? -un[k] : un[k]) - uref[k] : 0.f;
+              cc[k] = ok ? (rv[k] ? -cn : cn) : 0.f;
+            }
+            node_moments(v, d, cc);
+            contract_z(Gz, wz, all3, [&](int t) { return v[t]; }, Zc);
           }
+          float Gy[3][3];
+          basis_coeffs(ainv, bq[1], Gy);
+          contract_y(Gy, wy, all3, Zc, Yr);
         }
+        float Gx[3][3];
+        basis_coeffs(ainv, bq[0], Gx);
+        contract_x(Gx, wx, all3, Yr, acc);
       }
     }
     if (!done) {
@@ -393,11 +481,19 @@ __global__ void __launch_bounds__(THREADS, 1) pull_d3q27_tile_kernel(StepArgs<fl
 #pragma unroll
         for (int t = 0; t < 27; t++) acc[t] = 0.f;
       }
+      float f0[27];
+#pragma unroll
+      for (int t = 0; t < 27; t++) f0[t] = f0s[t * THREADS];
       conv = moments_and_test<POND_D3Q27, float>(a, acc, f0, C, rho0, U, T);
+#pragma unroll
+      for (int t = 0; t < 27; t++) f0s[t * THREADS] = f0[t];
       if (conv || niter >= a.max_iter) done = true;
     }
   }
   if (active) {
+    float f0[27];
+#pragma unroll
+    for (int t = 0; t < 27; t++) f0[t] = f0s[t * THREADS];
     finish_node<POND_D3Q27, float>(a, idx, f0, rho0, U, T, niter, conv, ns);
     ns.work = work;
   }
