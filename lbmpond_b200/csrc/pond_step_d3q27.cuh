@@ -10,15 +10,18 @@
 //    resolution (periodic wrap, clamp, mirror with population reversal), the
 //    reference's dropping of non-finite terms and the square root of T are
 //    applied while staging;
-//  * after staging, each staged node's 27 populations are replaced by its 27
-//    velocity moments V[k] = sum_b v_b^k f_b (k = 0..2 per axis) in a
-//    velocity frame shared by the CTA.  The transfer of a source node into
-//    the target gauge, sum_b prod_ax L_i(y_b) f_b with y = (v_b - U)/C and
-//    L_i the quadratic Lagrange basis over the target classes, is then
-//    sum_k G[i][k] V[k], where G depends on the target gauge only; so the
-//    interpolation weights and G are contracted against the moments one axis
-//    at a time (z per stencil node, y per stencil column, x per stencil row:
-//    81 FMA each) instead of transforming every stencil node (243 FMA);
+//  * after staging, each staged node's 27 populations are replaced by their
+//    transfer into a reference gauge shared by the CTA (the gauge of the
+//    tile's centre node).  The transfer of a source node into a target gauge
+//    (U, C), sum_b prod_ax L_i(y_b) f_b with y = (v_b - U)/C and L_i the
+//    quadratic Lagrange basis over the target classes, is a quadratic in the
+//    particle velocity v_b along each axis, so it equals the transfer from
+//    the reference gauge to (U, C), G[i][k] = L_i((u_ref + c_ref xi_k - U)/C),
+//    applied to the reference-gauge populations.  G depends on the target
+//    alone: the interpolation weights and G are contracted against the
+//    reference-gauge populations one axis at a time (z per stencil node, y
+//    per stencil column, x per stencil row: 81 FMA each) instead of
+//    transforming every stencil node into the target gauge (243 FMA);
 //  * the fixed-point iteration is warp-synchronous: a warp iterates while any
 //    of its lanes is unconverged, and walks the stencil offsets common to its
 //    lanes, so a warp's shared-memory loads hit 32 consecutive addresses;
@@ -53,49 +56,48 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // class index -> its mirror image along one axis (0 <-> 0, + <-> -)
 __device__ __forceinline__ int rev3(int c) { return c == 0 ? 0 : 3 - c; }
 
-// Velocity moments of one node along the three axes, in place over its 27
-// populations (tensor-class order, xi = {0, +1, -1} per axis):
-//   V[k1,k2,k3] = sum_b vx_b^k1 vy_b^k2 vz_b^k3 f_b,  v_b = d + c_ax xi_b,
-// with d = u - u_ref (a velocity frame shared by the CTA) and c_ax the
-// node's sqrts(T/TLat) (negated on a mirrored axis, which reverses the
-// classes along it).  Per axis: S = f+ + f-, D = f+ - f-,
-//   V0 = f0 + S,  V1 = d V0 + c D,  V2 = d V1 + c (d D + c S).
-__device__ __forceinline__ void node_moments(float v[27], const float d[3], const float c[3]) {
+// Quadratic Lagrange basis over the classes xi = {0, +1, -1}, evaluated at
+// s + r xi_b: B[i][b] = L_i(s + r xi_b) with L_0 = 1 - y^2,
+// L_+ = y (y + 1) / 2, L_- = y (y - 1) / 2.  B is the one-axis gauge
+// transfer (structs.cuh:343-551) from a gauge (u, c) to (U, C) for
+// s = (u - U) / C, r = c / C.
+__device__ __forceinline__ void basis_rows(float s, float r, float B[3][3]) {
+  const float y[3] = {s, s + r, s - r};
+#pragma unroll
+  for (int b = 0; b < 3; b++) {
+    const float yb = y[b], h = 0.5f * yb;
+    B[0][b] = fmaf(-yb, yb, 1.f);
+    B[1][b] = fmaf(h, yb, h);
+    B[2][b] = fmaf(h, yb, -h);
+  }
+}
+
+// Transfer of one node's 27 populations (tensor-class order), in place, into
+// the gauge (u_ref, c_ref) shared by the CTA: per axis the 3x3 basis with
+// s = (u - u_ref) / c_ref, r = c / c_ref.  A transfer into the target gauge
+// then equals the transfer of the result from (u_ref, c_ref) to the target,
+// because the basis reproduces every quadratic in the particle velocity.
+__device__ __forceinline__ void node_to_ref(float v[27], const float s[3], const float r[3]) {
 #pragma unroll
   for (int ax = 0; ax < 3; ax++) {
+    float B[3][3];
+    basis_rows(s[ax], r[ax], B);
     const int st = ax == 0 ? 9 : ax == 1 ? 3 : 1;
 #pragma unroll
     for (int o = 0; o < 9; o++) {
       // the two other axes' indices
       const int base = ax == 0 ? o : ax == 1 ? (o / 3) * 9 + (o % 3) : o * 3;
       const float f0 = v[base], fp = v[base + st], fm = v[base + 2 * st];
-      const float S = fp + fm, D = fp - fm;
-      const float V0 = f0 + S;
-      const float V1 = fmaf(d[ax], V0, c[ax] * D);
-      const float V2 = fmaf(d[ax], V1, c[ax] * fmaf(d[ax], D, c[ax] * S));
-      v[base] = V0; v[base + st] = V1; v[base + 2 * st] = V2;
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        const float o3 = fmaf(B[i][2], fm, fmaf(B[i][1], fp, B[i][0] * f0));
+        if (i == 0) v[base] = o3; else if (i == 1) v[base + st] = o3; else v[base + 2 * st] = o3;
+      }
     }
   }
 }
 
-// Basis coefficients of one axis for a target gauge (U, C): the Lagrange
-// basis polynomials over the target classes, L_0 = 1 - y^2,
-// L_+ = y (y + 1) / 2, L_- = y (y - 1) / 2, at y = (v - (U - u_ref)) / C
-// = a v + b, expanded in powers of v: L_i(y) = sum_k G[i][k] v^k.
-__device__ __forceinline__ void basis_coeffs(float a, float b, float G[3][3]) {
-  const float a2 = a * a;
-  G[0][0] = fmaf(-b, b, 1.f);
-  G[0][1] = -2.f * a * b;
-  G[0][2] = -a2;
-  G[1][0] = 0.5f * fmaf(b, b, b);
-  G[1][1] = a * (b + 0.5f);
-  G[1][2] = 0.5f * a2;
-  G[2][0] = 0.5f * fmaf(b, b, -b);
-  G[2][1] = a * (b - 0.5f);
-  G[2][2] = 0.5f * a2;
-}
-
-// Z[k1,k2,i3] += sum_k3 w_i3 Gz[i3][k3] V[k1,k2,k3] for the z-classes i3
+// Z[k1,k2,i3] += sum_k3 w_i3 Gz[i3][k3] F[k1,k2,k3] (F: reference-gauge populations) for the z-classes i3
 // flagged in nz (the first contraction, one per stencil node).
 template <typename LoadV>
 __device__ __forceinline__ void contract_z(const float Gz[3][3], const float wz[3], const bool nz[3], LoadV loadv,
@@ -269,15 +271,19 @@ __global__ void __launch_bounds__(THREADS, 1) pull_d3q27_tile_kernel(StepArgs<fl
     flags[i] = (unsigned char)(fl | (ok ? 0 : 8));
   }
   __syncthreads();
-  // 4) velocity frame of the CTA: the gauge of the tile's centre node
-  float uref[3];
+  // 4) reference gauge of the CTA: the gauge of the tile's centre node
+  //    (c = 1 if that node's c is 0)
+  float uref[3], icref;
   {
     constexpr int ci = (H + TZ / 2) * SX * SY + (H + TY / 2) * SX + (H + TX / 2);
 #pragma unroll
     for (int k = 0; k < 3; k++) uref[k] = sm[(27 + k) * SN + ci];
+    const float cc = sm[30 * SN + ci];
+    icref = fabsf(cc) > 1.0e-20f ? 1.f / cc : 1.f;
   }
-  // 5) populations -> velocity moments in that frame, in place (non-finite
-  //    populations and every population of an invalid node count as 0)
+  const float cref = 1.f / icref;
+  // 5) populations -> transferred into the reference gauge, in place
+  //    (non-finite populations and every population of an invalid node count as 0)
   for (int i = tid; i < SN; i += THREADS) {
     const bool bad = flags[i] & 8;
     float v[27];
@@ -286,10 +292,11 @@ __global__ void __launch_bounds__(THREADS, 1) pull_d3q27_tile_kernel(StepArgs<fl
       const float x = sm[t * SN + i];
       v[t] = (!bad && fabsf(x) <= 3.402823466e38f) ? x : 0.f;
     }
-    const float c = sm[30 * SN + i];
-    const float d[3] = {sm[27 * SN + i] - uref[0], sm[28 * SN + i] - uref[1], sm[29 * SN + i] - uref[2]};
-    const float cc[3] = {c, c, c};
-    node_moments(v, d, cc);
+    const float r = sm[30 * SN + i] * icref;
+    const float sq[3] = {(sm[27 * SN + i] - uref[0]) * icref, (sm[28 * SN + i] - uref[1]) * icref,
+                         (sm[29 * SN + i] - uref[2]) * icref};
+    const float rq[3] = {r, r, r};
+    node_to_ref(v, sq, rq);
 #pragma unroll
     for (int t = 0; t < 27; t++) sm[t * SN + i] = v[t];
   }
@@ -341,13 +348,14 @@ __global__ void __launch_bounds__(THREADS, 1) pull_d3q27_tile_kernel(StepArgs<fl
       lo[ax] = min(ro[ax][0], min(ro[ax][1], ro[ax][2]));
       hi[ax] = max(ro[ax][0], max(ro[ax][1], ro[ax][2])) + N - 1;
     }
-    // basis coefficients per axis: y = (v + u_ref - U) / C = a v + b
-    const float ainv = __frcp_rn(float(C));
+    // transfer from the reference gauge to this iteration's target gauge,
+    // per axis: G[i][k] = L_i(b + a xi_k), a = c_ref / C, b = (u_ref - U) / C
+    const float ainv = float(double(cref) / C);
     float bq[3];
 #pragma unroll
     for (int ax = 0; ax < 3; ax++) bq[ax] = float((double(uref[ax]) - U[ax]) / C);
     float Gz[3][3];  // the z basis is used per stencil node; x and y are rebuilt per row and column
-    basis_coeffs(ainv, bq[2], Gz);
+    basis_rows(bq[2], ainv, Gz);
     float acc[27];
 #pragma unroll
     for (int t = 0; t < 27; t++) acc[t] = 0.f;
@@ -412,11 +420,11 @@ __global__ void __launch_bounds__(THREADS, 1) pull_d3q27_tile_kernel(StepArgs<fl
             contract_z(Gz, wz, nz, [&](int t) { return sv[t * SN]; }, Zc);
           }
           float Gy[3][3];
-          basis_coeffs(ainv, bq[1], Gy);
+          basis_rows(bq[1], ainv, Gy);
           contract_y(Gy, wy, ny, Zc, Yr);
         }
         float Gx[3][3];
-        basis_coeffs(ainv, bq[0], Gx);
+        basis_rows(bq[0], ainv, Gx);
         contract_x(Gx, wx, nx, Yr, acc);
       }
     } else if (!done) {
@@ -457,21 +465,21 @@ __global__ void __launch_bounds__(THREADS, 1) pull_d3q27_tile_kernel(StepArgs<fl
 #pragma unroll
             for (int t = 0; t < 27; t++)
               v[t] = ok ? finite_or_zero_f(__ldg(&a.f_in[(long long)c_ref27[t] * a.N + g])) : 0.f;
-            float d[3], cc[3];
+            float sq[3], rq[3];
 #pragma unroll
             for (int k = 0; k < 3; k++) {
-              d[k] = ok ? (rv[k] ? -un[k] : un[k]) - uref[k] : 0.f;
-              cc[k] = ok ? (rv[k] ? -cn : cn) : 0.f;
+              sq[k] = ok ? ((rv[k] ? -un[k] : un[k]) - uref[k]) * icref : 0.f;
+              rq[k] = ok ? (rv[k] ? -cn : cn) * icref : 0.f;
             }
-            node_moments(v, d, cc);
+            node_to_ref(v, sq, rq);
             contract_z(Gz, wz, all3, [&](int t) { return v[t]; }, Zc);
           }
           float Gy[3][3];
-          basis_coeffs(ainv, bq[1], Gy);
+          basis_rows(bq[1], ainv, Gy);
           contract_y(Gy, wy, all3, Zc, Yr);
         }
         float Gx[3][3];
-        basis_coeffs(ainv, bq[0], Gx);
+        basis_rows(bq[0], ainv, Gx);
         contract_x(Gx, wx, all3, Yr, acc);
       }
     }
