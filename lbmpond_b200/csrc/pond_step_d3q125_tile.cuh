@@ -1,24 +1,32 @@
 // D3Q125 PonD pull step, float32: a tile of nodes per CTA, a warp per node.
 //
 // Same arithmetic as pull_d3q125_kernel (steps.cu:151-250 PonDstepD3Q125:
-// quadratic stencil with its origin fixed at coord-1, separable gauge
-// transform with the interpolation weights folded into the basis rows,
-// float64 moments and convergence test), organised for the SM:
+// quadratic stencil with its origin fixed at coord-1, gauge transfer by the
+// 5-point Lagrange basis, float64 moments and convergence test), organised
+// for the SM:
 //
 //  * a CTA owns a 4 x 4 x 4 tile and stages it with its +-1 halo (6 x 6 x 6
 //    nodes: 125 population planes, the gauge velocities and c, 113 KB) once
 //    per step, so two CTAs fit on an SM and every staged node serves up to
 //    27 centres from shared memory;
+//  * after staging, one thread per staged node transfers its populations
+//    into a reference gauge R shared by the CTA (the gauge of a tile node):
+//    three passes of the 5x5 basis.  The transfer of a source node into a
+//    target gauge is, along each axis, a quartic in the particle velocity,
+//    which the 5-point basis reproduces, so it equals the transfer R ->
+//    target applied to the R-gauge populations; R -> target depends on the
+//    target alone;
 //  * each of the 8 warps takes 8 nodes of the tile in turn and iterates one
-//    node at a time, so a warp never waits for another node's iterations;
-//  * lane 5j+k (25 lanes) owns source x-class j and target z-class k: per
-//    stencil node it runs the z pass (t1[j][*][k], 25 FMA) and the y pass
-//    (t2[j][*][k], 25 FMA) on its own data, then takes t2 of the lanes with
-//    the same k by shuffle and accumulates target populations (j, *, k) of
-//    the x pass (25 FMA); the 75 weighted basis entries of the stencil node
-//    are computed three per lane into a per-warp table;
+//    node at a time.  Lane 5p+q (25 lanes) owns R-class p along x and target
+//    class q along z: per stencil node it contracts the z weights and
+//    transfer against the R-gauge populations (p, *, *) (25 FMA), per stencil
+//    column the y weights and transfer (25 FMA, coefficients from a per-warp
+//    table), and per stencil row the x weights and transfer of its target
+//    x-class p against the column results of the lanes (*, q) by shuffle
+//    (25 FMA): 1,125 FMA per lane and iteration where the per-node transform
+//    takes 2,025;
 //  * the plane stride of the staged populations is 217 slots, so the five
-//    source x-classes read in one instruction fall in distinct banks.
+//    R x-classes read in one instruction fall in distinct banks.
 // Mirrored axes are handled as in the reference kernel: the staged node's
 // velocity component and c flip sign along that axis (-c maps each
 // population onto its mirror image), the populations stay in place.
@@ -37,11 +45,11 @@ constexpr int WARPS = 8;
 constexpr int THREADS = 32 * WARPS;
 
 struct Smem {
-  float f[125 * PS];       // staged populations, non-finite values zeroed
+  float f[125 * PS];       // staged populations (non-finite values zeroed), then their transfer into R
   float u[3][SN];          // staged velocities (sign-flipped on mirrored axes)
   float c[SN];             // sqrts(T / TLat)
   unsigned char flags[SN]; // mirrored axes (bits 0-2)
-  float M[WARPS][3][6][5]; // per-warp weighted basis rows of the current stencil node (row 5: idle lanes)
+  float GY[WARPS][3][25];  // per warp and iteration: y weight x transfer entry, [n_y][5 i2 + k2]
 };
 
 static_assert(2 * (sizeof(Smem) + 1024) <= 233472, "two CTAs must fit in the 228 KB of an SM");
@@ -74,6 +82,16 @@ struct BasisRow {
 };
 
 __device__ __forceinline__ double xi5(int c) { return Lattice<POND_D3Q125>::xi1(c); }
+__device__ __forceinline__ float xi5f(int c) {
+  return c == 0 ? 0.f : c == 1 ? float(EC1) : c == 2 ? -float(EC1) : c == 3 ? float(EC2) : -float(EC2);
+}
+
+// LagrPol<3> factors of target class cls along one axis at the three stencil
+// positions coord-1, coord, coord+1 (steps.cu:151-250 fixed-origin quadratic)
+__device__ __forceinline__ void stencil_weights(int pos, double C, double U, int cls, float w[3]) {
+  const double crd = double(pos) - (C * xi5(cls) + U);
+  lagr_weights<3, float>(crd - double(pos - 1), w);
+}
 
 __global__ void __launch_bounds__(THREADS, 2) pull_d3q125_tile_kernel(StepArgs<float> a) {
   using L = Lattice<POND_D3Q125>;
@@ -112,12 +130,80 @@ __global__ void __launch_bounds__(THREADS, 2) pull_d3q125_tile_kernel(StepArgs<f
   }
   __syncthreads();
 
-  // ---- one warp per node; lane 5j+k: source / target x-class j, z-class k
-  // idle lanes (25..31) compute like lane 20+k and write table row 5, which nobody reads
+  // ---- reference gauge R: the staged node at tile position (2, 2, 2)
+  //      ((0, 1) if that node's gauge is not finite or its c is 0)
+  float uref[3], cref;
+  {
+    constexpr int ci = ((2 + 1) * S + (2 + 1)) * S + (2 + 1);
+    const float cc = sm.c[ci];
+    bool ok = fabsf(cc) <= 3.0e38f && fabsf(cc) > 1.0e-20f;
+#pragma unroll
+    for (int ax = 0; ax < 3; ax++) {
+      uref[ax] = sm.u[ax][ci];
+      ok = ok && fabsf(uref[ax]) <= 3.0e38f;
+    }
+#pragma unroll
+    for (int ax = 0; ax < 3; ax++) uref[ax] = ok ? uref[ax] : 0.f;
+    cref = ok ? cc : 1.f;
+  }
+  // ---- every staged node into R, one thread per node, three passes of the
+  //      5x5 basis B[i][b] = L_i(s + r xi_b), s = (u - u_ref)/c_ref,
+  //      r = +-c/c_ref; a node with a non-finite gauge contributes nothing
+  {
+    const float icref = 1.f / cref;
+    for (int i = tid; i < SN; i += THREADS) {
+      const unsigned fl = sm.flags[i];
+      const float cn = sm.c[i];
+      bool ok = fabsf(cn) <= 3.0e38f;
+      float sq[3], rq[3];
+#pragma unroll
+      for (int ax = 0; ax < 3; ax++) {
+        const float un = sm.u[ax][i];
+        ok = ok && fabsf(un) <= 3.0e38f;
+        sq[ax] = (un - uref[ax]) * icref;
+        rq[ax] = ((fl >> ax) & 1 ? -cn : cn) * icref;
+      }
+      float* fi = sm.f + i;
+      if (!ok) {
+        for (int pp = 0; pp < 125; pp++) fi[pp * PS] = 0.f;
+        continue;
+      }
+#pragma unroll
+      for (int ax = 0; ax < 3; ax++) {
+        float B[5][5];
+#pragma unroll
+        for (int ii = 0; ii < 5; ii++) {
+          const BasisRow Li(ii);
+#pragma unroll
+          for (int b = 0; b < 5; b++) B[ii][b] = finite_or_zero_f(Li(fmaf(rq[ax], xi5f(b), sq[ax])));
+        }
+        const int st = ax == 0 ? 25 : ax == 1 ? 5 : 1;
+#pragma unroll 5
+        for (int o = 0; o < 25; o++) {
+          const int base = ax == 0 ? o : ax == 1 ? 25 * (o / 5) + o % 5 : 5 * o;
+          float v[5], w[5];
+#pragma unroll
+          for (int b = 0; b < 5; b++) v[b] = fi[(base + b * st) * PS];
+#pragma unroll
+          for (int ii = 0; ii < 5; ii++) {
+            float t = B[ii][0] * v[0];
+#pragma unroll
+            for (int b = 1; b < 5; b++) t = fmaf(B[ii][b], v[b], t);
+            w[ii] = t;
+          }
+#pragma unroll
+          for (int ii = 0; ii < 5; ii++) fi[(base + ii * st) * PS] = w[ii];
+        }
+      }
+    }
+  }
+  __syncthreads();
+
+  // ---- one warp per node; lane 5p+q: R x-class p (target x-class p for the
+  // output), target z-class q.  Idle lanes (25..31) compute like lane 20+q and
+  // write nothing.
   const bool worker = lane < 25;
-  const int j = worker ? lane / 5 : 4, k = lane % 5, jrow = worker ? j : 5;
-  const BasisRow Lj(j);
-  const float xik = float(xi5(k));
+  const int j = worker ? lane / 5 : 4, k = lane % 5;
   NodeSums ns = {0, 0, 0, 0, 0, 0, 0ull, 0ull, 0ull, 0};
   for (int t = warp; t < T * T * T; t += WARPS) {
     const int lx = t % T, ly = (t / T) % T, lz = t / (T * T);
@@ -148,67 +234,70 @@ __global__ void __launch_bounds__(THREADS, 2) pull_d3q125_tile_kernel(StepArgs<f
     while (niter < a.max_iter) {
       niter++;
       const double C = sqrt(Tc / L::TLat);
-      const float invC = __frcp_rn(float(C));
-      // LagrPol<3> factors of target class j (this lane's basis row) per
-      // axis at the three stencil positions: shift = crd - (coord - 1)
-      float w3[3][3];
+      // transfer R -> target per axis: G[i][k] = L_i(b + a xi_k), a = c_ref/C, b = (u_ref - U)/C
+      const float ga = float(double(cref) / C);
+      float gb[3];
 #pragma unroll
-      for (int ax = 0; ax < 3; ax++) {
-        const double crd = double(pos[ax]) - (C * xi5(j) + U[ax]);
-        lagr_weights<3, float>(crd - double(pos[ax] - 1), w3[ax]);
+      for (int ax = 0; ax < 3; ax++) gb[ax] = float((double(uref[ax]) - U[ax]) / C);
+      // this lane's z (class k) and x (class j) transfer rows and stencil weights
+      float tz[5], tx[5], wz[3], wx[3];
+      stencil_weights(pos[2], C, U[2], k, wz);
+      stencil_weights(pos[0], C, U[0], j, wx);
+      const BasisRow Lj(j), Lk(k);
+#pragma unroll
+      for (int kk = 0; kk < 5; kk++) {
+        tz[kk] = finite_or_zero_f(Lk(fmaf(ga, xi5f(kk), gb[2])));
+        tx[kk] = finite_or_zero_f(Lj(fmaf(ga, xi5f(kk), gb[0])));
       }
-      const float Uf[3] = {float(U[0]), float(U[1]), float(U[2])};
+      // y coefficients of every (n_y, i2, k2): three table entries per worker lane
+      __syncwarp();  // the previous iteration's readers are done with the table
+      if (worker) {
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+          const int e = 3 * lane + r, ny = e / 25, i2 = (e / 5) % 5, k2 = e % 5;
+          float wy[3];
+          stencil_weights(pos[1], C, U[1], i2, wy);
+          const float ty = finite_or_zero_f(BasisRow(i2)(fmaf(ga, xi5f(k2), gb[1])));
+          sm.GY[warp][ny][5 * i2 + k2] = (ny == 0 ? wy[0] : ny == 1 ? wy[1] : wy[2]) * ty;
+        }
+      }
+      __syncwarp();
 #pragma unroll
       for (int iy = 0; iy < 5; iy++) acc[iy] = 0.f;
-      for (int n = 0; n < 27; n++) {
-        const int na[3] = {n / 9, (n / 3) % 3, n % 3};
-        const int q = qc + (na[2] - 1) * S * S + (na[1] - 1) * S + (na[0] - 1);
-        // this lane's three basis entries M[ax][j][k] = w_j L_j(s + r xi_k)
-        {
-          const float cq = sm.c[q] * invC;
-          const unsigned fl = sm.flags[q];
 #pragma unroll
-          for (int ax = 0; ax < 3; ax++) {
-            const float s = (sm.u[ax][q] - Uf[ax]) * invC;
-            const float r = (fl >> ax) & 1 ? -cq : cq;
-            const float wj = na[ax] == 0 ? w3[ax][0] : na[ax] == 1 ? w3[ax][1] : w3[ax][2];
-            sm.M[warp][ax][jrow][k] = wj * finite_or_zero_f(Lj(fmaf(r, xik, s)));
+      for (int nx = 0; nx < 3; nx++) {
+        float Yr[5] = {0.f, 0.f, 0.f, 0.f, 0.f};  // (j, i2, k) of the row
+#pragma unroll 1
+        for (int ny = 0; ny < 3; ny++) {
+          float Zc[5] = {0.f, 0.f, 0.f, 0.f, 0.f};  // (j, k2, k) of the column
+#pragma unroll 1
+          for (int nz = 0; nz < 3; nz++) {
+            const float wn = nz == 0 ? wz[0] : nz == 1 ? wz[1] : wz[2];
+            float gz[5];
+#pragma unroll
+            for (int k3 = 0; k3 < 5; k3++) gz[k3] = wn * tz[k3];
+            const float* fq = sm.f + (25 * j) * PS + qc + (nz - 1) * S * S + (ny - 1) * S + (nx - 1);
+#pragma unroll
+            for (int k2 = 0; k2 < 5; k2++)
+#pragma unroll
+              for (int k3 = 0; k3 < 5; k3++) Zc[k2] = fmaf(gz[k3], fq[(5 * k2 + k3) * PS], Zc[k2]);
           }
+          const float* gy = sm.GY[warp][ny];
+#pragma unroll
+          for (int i2 = 0; i2 < 5; i2++)
+#pragma unroll
+            for (int k2 = 0; k2 < 5; k2++) Yr[i2] = fmaf(gy[5 * i2 + k2], Zc[k2], Yr[i2]);
         }
-        __syncwarp();
-        // z pass: t1[jy] = sum_jz Mz[k][jz] f[j][jy][jz]
-        float mz[5];
 #pragma unroll
-        for (int jz = 0; jz < 5; jz++) mz[jz] = sm.M[warp][2][k][jz];
-        float t1[5];
-        const float* fq = sm.f + (25 * j) * PS + q;
+        for (int k1 = 0; k1 < 5; k1++) {
+          const float g = wx[nx] * tx[k1];
 #pragma unroll
-        for (int jy = 0; jy < 5; jy++) {
-          float v = 0.f;
-#pragma unroll
-          for (int jz = 0; jz < 5; jz++) v += mz[jz] * fq[(5 * jy + jz) * PS];
-          t1[jy] = v;
+          for (int i2 = 0; i2 < 5; i2++) acc[i2] = fmaf(g, __shfl_sync(0xffffffffu, Yr[i2], 5 * k1 + k), acc[i2]);
         }
-        // y pass: t2[iy] = sum_jy My[iy][jy] t1[jy]
-        float t2[5];
+      }
+      if (!(C >= 1.0e-300)) {  // target T = 0: every transfer term is non-finite and dropped
 #pragma unroll
-        for (int iy = 0; iy < 5; iy++) {
-          float v = 0.f;
-#pragma unroll
-          for (int jy = 0; jy < 5; jy++) v += sm.M[warp][1][iy][jy] * t1[jy];
-          t2[iy] = v;
-        }
-        // x pass: acc[iy] += sum_jx Mx[j][jx] t2 of lane (jx, k)
-        float mxr[5];
-#pragma unroll
-        for (int jx = 0; jx < 5; jx++) mxr[jx] = sm.M[warp][0][j][jx];
-#pragma unroll
-        for (int jx = 0; jx < 5; jx++) {
-          const float mx = mxr[jx];
-#pragma unroll
-          for (int iy = 0; iy < 5; iy++) acc[iy] += mx * __shfl_sync(0xffffffffu, t2[iy], 5 * jx + k);
-        }
-        __syncwarp();  // the table is rewritten for the next stencil node
+        for (int iy = 0; iy < 5; iy++) acc[iy] = 0.f;
       }
       // calcMoments in float64 (structs.cuh:315-342), warp-wide
       double mv[5] = {0, 0, 0, 0, 0};
