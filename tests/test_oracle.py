@@ -75,6 +75,29 @@ def test_transfer_gauge_preserves_moments(orc, lat, seed):
 
 
 @pytest.mark.parametrize("lat", LATS)
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_transfer_through_reference_gauge(orc, lat, seed):
+    """The tile kernels transfer every staged node once per step into a
+    reference gauge R and, per iteration, apply the transfer R -> target.
+    That equals the direct transfer source -> target because the Lagrange
+    basis of the transfer reproduces the polynomials it is built from;
+    checked here on the reference's own transfer (transfer_gauge)."""
+    t = orc.tables(lat)
+    rng = np.random.default_rng(10 + seed)
+    f = t.w * (1 + 0.2 * rng.standard_normal(t.Q))
+    d3 = t.dim == 3
+
+    def gauge():
+        return np.array([rng.uniform(-.1, .1), rng.uniform(-.1, .1) * d3, rng.uniform(-.1, .1) * d3,
+                         rng.uniform(.05, .2)])
+    src, ref, dst = gauge(), gauge(), gauge()
+    direct = np.array([orc.transfer_gauge(lat, f, src, dst, i) for i in range(t.Q)])
+    f_ref = np.array([orc.transfer_gauge(lat, f, src, ref, i) for i in range(t.Q)])
+    via = np.array([orc.transfer_gauge(lat, f_ref, ref, dst, i) for i in range(t.Q)])
+    assert np.allclose(via, direct, rtol=1e-10, atol=1e-13 * np.abs(f).max())
+
+
+@pytest.mark.parametrize("lat", LATS)
 def test_set_base_and_moments(orc, lat):
     t = orc.tables(lat)
     uT = [0.03, -0.02 if t.dim == 3 else 0, 0.01 if t.dim == 3 else 0, 0.12]
