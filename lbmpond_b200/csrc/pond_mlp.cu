@@ -484,14 +484,21 @@ int run_predictor(pond_ctx* c) {
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->p.device);
   const long long tiles = (c->N + 127) / 128;
-  const int grid = (int)std::min<long long>(tiles, (long long)nsm * 4);
   const size_t smem = infer_smem(m->H);
   const int cu = c->cur;
   const float gate = c->gate;
   cudaError_t e;
+  int grid = 0;
+  // one wave: every CTA resident at once (the grid-stride loop gives each the same share)
 #define POND_PREDICT(HH, RR)                                                                                       \
   e = cudaFuncSetAttribute(mlp::predict_kernel<HH, RR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);   \
   if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");                                               \
+  {                                                                                                                \
+    int per_sm = 1;                                                                                                \
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mlp::predict_kernel<HH, RR>, 128, smem);            \
+    if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");                    \
+    grid = (int)std::min<long long>(tiles, (long long)nsm * std::max(per_sm, 1));                                  \
+  }                                                                                                                \
   mlp::predict_kernel<HH, RR><<<grid, 128, smem, c->stream>>>(m->P, m->stats, (const RR*)c->rho[cu],               \
                                                               (const RR*)c->g[cu], (const RR*)c->g[1 - cu], c->N,   \
                                                               (int)c->p.Nx,                                        \
