@@ -43,6 +43,7 @@ class _Params(ctypes.Structure):
         ("tol_rel", ctypes.c_double),
         ("max_iter", ctypes.c_int),
         ("nthreads", ctypes.c_int),
+        ("dof", ctypes.c_double),
     ]
 
 
@@ -77,6 +78,9 @@ def lib():
         L.orc_lagr_pol.restype = ctypes.c_double
         L.orc_step.argtypes = [ctypes.POINTER(_Params), dp, dp, dp, dp, dp, dp, dp, ip]
         L.orc_step.restype = ctypes.c_int64
+        L.orc_set_energy.argtypes = [ctypes.c_int, ctypes.c_double, dp, ctypes.c_double, dp]
+        L.orc_step_ddf.argtypes = [ctypes.POINTER(_Params), dp, dp, dp, dp, dp, dp, dp, dp, dp, ip]
+        L.orc_step_ddf.restype = ctypes.c_int64
         L.orc_max_threads.restype = ctypes.c_int
         _lib = L
     return _lib
@@ -144,14 +148,35 @@ def lagr_pol(n, ix, iy, iz, sx, sy, sz) -> float:
     return lib().orc_lagr_pol(n, ix, iy, iz, sx, sy, sz)
 
 
+def set_energy(lattice: int, rho: float, uT, dof: float) -> np.ndarray:
+    """Equilibrium energy populations of one node (double-distribution
+    extension): h_i = rho w_i (|v_i|^2 + dof T)."""
+    L = lib()
+    h = np.zeros(L.orc_q(lattice))
+    u = np.ascontiguousarray(uT, dtype=np.float64)
+    L.orc_set_energy(lattice, float(rho), _dp(u), float(dof), _dp(h))
+    return h
+
+
 @dataclass
 class State:
     f: np.ndarray    # [Q, N]
     rho: np.ndarray  # [N]
     g: np.ndarray    # [4, N]
+    h: np.ndarray | None = None  # [Q, N] energy populations (double-distribution extension)
 
     def copy(self):
-        return State(self.f.copy(), self.rho.copy(), self.g.copy())
+        return State(self.f.copy(), self.rho.copy(), self.g.copy(), None if self.h is None else self.h.copy())
+
+
+def with_energy(state: State, lattice: int, dof: float) -> State:
+    """The state plus equilibrium energy populations in every node's gauge."""
+    t = tables(lattice)
+    rho, g = state.rho, state.g
+    s = np.sqrt(np.abs(g[3]) / t.tlat)
+    v2 = sum((s[None, :] * t.xi[:, a:a + 1] + g[a][None, :]) ** 2 for a in range(3))
+    h = t.w[:, None] * rho[None, :] * (v2 + dof * g[3][None, :])
+    return State(state.f.copy(), rho.copy(), g.copy(), np.ascontiguousarray(h))
 
 
 def base_state(lattice: int, rho, ux, uy, uz, T) -> State:
@@ -165,16 +190,21 @@ def base_state(lattice: int, rho, ux, uy, uz, T) -> State:
 
 
 def step(state: State, lattice: int, shape, interp=None, tau=0.9, tol_abs=1e-12, tol_rel=1e-10,
-         max_iter=100, bc=(BC_PERIODIC,) * 3, guess=None, nthreads=0):
-    """One pull step; returns (new_state, niter[N], nonconverged_count)."""
+         max_iter=100, bc=(BC_PERIODIC,) * 3, guess=None, nthreads=0, dof=None):
+    """One pull step; returns (new_state, niter[N], nonconverged_count).  A
+    state with energy populations (``state.h``) steps with the
+    double-distribution extension and needs ``dof``."""
     L = lib()
     nx, ny, nz = shape
     N = nx * ny * nz
     Q = L.orc_q(lattice)
     if interp is None:
         interp = DEFAULT_INTERP[lattice]
+    ddf = state.h is not None
+    if ddf and dof is None:
+        raise ValueError("a state with energy populations needs dof")
     p = _Params(lattice, interp, nx, ny, nz, (ctypes.c_int * 3)(*bc), tau, tol_abs, tol_rel,
-                max_iter, nthreads)
+                max_iter, nthreads, float(dof) if ddf else 0.0)
     f_in = np.ascontiguousarray(state.f, dtype=np.float64)
     r_in = np.ascontiguousarray(state.rho, dtype=np.float64)
     g_in = np.ascontiguousarray(state.g, dtype=np.float64)
@@ -186,8 +216,15 @@ def step(state: State, lattice: int, shape, interp=None, tau=0.9, tol_abs=1e-12,
         guess = np.ascontiguousarray(guess, dtype=np.float64)
         assert guess.shape == (4, N)
         gp = _dp(guess)
-    nc = L.orc_step(ctypes.byref(p), _dp(f_in), _dp(r_in), _dp(g_in), gp,
-                    _dp(out.f), _dp(out.rho), _dp(out.g), _ip(niter))
+    if ddf:
+        h_in = np.ascontiguousarray(state.h, dtype=np.float64)
+        assert h_in.shape == (Q, N)
+        out.h = np.empty((Q, N))
+        nc = L.orc_step_ddf(ctypes.byref(p), _dp(f_in), _dp(h_in), _dp(r_in), _dp(g_in), gp,
+                            _dp(out.f), _dp(out.h), _dp(out.rho), _dp(out.g), _ip(niter))
+    else:
+        nc = L.orc_step(ctypes.byref(p), _dp(f_in), _dp(r_in), _dp(g_in), gp,
+                        _dp(out.f), _dp(out.rho), _dp(out.g), _ip(niter))
     if nc < 0:
         raise ValueError("oracle step rejected its parameters")
     return out, niter, int(nc)

@@ -129,6 +129,7 @@ inline bool finite(double v) { return !std::isnan(v) && !std::isinf(v); }
 
 struct Cell {
   double f[QMAX];
+  double h[QMAX];  // energy populations of the double-distribution extension (unused otherwise)
   double rho;
   double uT[4];
 };
@@ -140,10 +141,31 @@ void set_base(const Lattice& L, Cell& c, double r, const double* uT) {
   for (int i = 0; i < L.Q; i++) c.f[i] = L.w[i] * c.rho;
 }
 
+// Equilibrium energy populations of the double-distribution extension in the
+// gauge uT: h_i = rho w_i (|v_i|^2 + dof T), v_i = sqrt(T/TLat) xi_i + u, so
+// that sum_i h_i = rho (|u|^2 + (Dim + dof) T) (twice the total energy) and
+// sum_i h_i v_i = rho u (|u|^2 + (Dim + 2 + dof) T) (twice the enthalpy flux).
+// The reference's scaffolding (lbpack.cu:18-20, steps.cu:233-236) uses
+// rho w_i (Dim T + |u|^2), whose flux lacks the pressure work.
+void set_energy(const Lattice& L, Cell& c, double dof) {
+  const double s = std::sqrt(std::fabs(c.uT[3]) / L.TLat);
+  for (int i = 0; i < L.Q; i++) {
+    double v2 = 0;
+    for (int a = 0; a < 3; a++) {
+      const double v = s * L.xi[i][a] + c.uT[a];
+      v2 += v * v;
+    }
+    c.h[i] = c.rho * L.w[i] * (v2 + dof * c.uT[3]);
+  }
+}
+
 // structs.cuh:343-551 Cell::transfer_gauge: population inew of cell c
 // re-expressed in the gauge `base` = (u1, T1).  Non-finite terms are dropped
-// (:390, :516, :542).
-double transfer_gauge(const Lattice& L, const Cell& c, const double* base, int inew) {
+// (:390, :516, :542).  `energy` transfers the energy populations h instead of
+// f (the reference's DDF branch, structs.cuh:391-394, applies the same
+// transfer to h).
+double transfer_gauge(const Lattice& L, const Cell& c, const double* base, int inew, bool energy = false) {
+  const double* src = energy ? c.h : c.f;
   const double Tbase = L.TLat;
   const double u0x = c.uT[0], u0y = c.uT[1], u0z = c.uT[2];
   const double T0 = c.uT[3];
@@ -186,7 +208,7 @@ double transfer_gauge(const Lattice& L, const Cell& c, const double* base, int i
       difM4moment *= 0;
       const double gx = K4 * difu * difu * difu * difu + K3 * difu * difu * difu + K2 * difu * difu +
                         K1 * difu + K0 - difM4moment;
-      const double fadd = wk * gx * c.f[iold];
+      const double fadd = wk * gx * src[iold];
       if (finite(fadd)) fnew += fadd;
     }
   } else if (L.kind == ORC_D3Q125) {  // :396-524
@@ -220,7 +242,7 @@ double transfer_gauge(const Lattice& L, const Cell& c, const double* base, int i
       const double gy = fY[(Yi + 1) % 5] * fY[(Yi + 2) % 5] * fY[(Yi + 3) % 5] * fY[(Yi + 4) % 5];
       const double gz = fZ[(Zi + 1) % 5] * fZ[(Zi + 2) % 5] * fZ[(Zi + 3) % 5] * fZ[(Zi + 4) % 5];
       const double gxyz = gx * gy * gz;
-      const double fadd = wk * wl * wm * gxyz * c.f[iold];
+      const double fadd = wk * wl * wm * gxyz * src[iold];
       if (finite(fadd)) fnew += fadd;
     }
   } else {  // generic branch :525-548 (D3Q27)
@@ -242,8 +264,8 @@ double transfer_gauge(const Lattice& L, const Cell& c, const double* base, int i
       const double gy = Ay_j * Ay_j - By_jl;
       const double gz = Az_p * Az_p - Bz_pm;
       double fadd = 0;
-      if (L.Dim == 1) fadd = wk * gx * c.f[iold];
-      else fadd = wk * wl * wm * gx * gy * gz * c.f[iold];
+      if (L.Dim == 1) fadd = wk * gx * src[iold];
+      else fadd = wk * wl * wm * gx * gy * gz * src[iold];
       if (finite(fadd)) fnew += fadd;
     }
   }
@@ -268,11 +290,14 @@ void calc_moments(const Lattice& L, Cell& c, const double (*vi)[3]) {
 }
 
 // steps.cu:58-75 isConv
-bool is_conv(const Lattice& L, const Cell& cnew, const Cell& cold, double ea, double er) {
+bool is_conv(const Lattice& L, const Cell& cnew, const Cell& cold, double ea, double er, bool ddf = false) {
   for (int k = 0; k < 4; k++)
     if (std::fabs(cnew.uT[k] - cold.uT[k]) >= ea + er * std::fabs(cnew.uT[k])) return false;
   for (int i = 0; i < L.Q; i++)
     if (std::fabs(cnew.f[i] - cold.f[i]) >= ea + er * std::fabs(cnew.f[i])) return false;
+  if (ddf)  // the energy populations converge like the others
+    for (int i = 0; i < L.Q; i++)
+      if (std::fabs(cnew.h[i] - cold.h[i]) >= ea + er * std::fabs(cnew.h[i])) return false;
   return true;
 }
 
@@ -296,6 +321,7 @@ double lin_pol(int ix, int iy, int iz, double sx, double sy, double sz) {
 struct Domain {
   const Lattice* L;
   const double* f;
+  const double* h;  // energy populations (nullptr without the double-distribution extension)
   const double* rho;
   const double* g;
   int64_t n[3];
@@ -328,6 +354,7 @@ void load_cell(const Domain& D, int64_t px, int64_t py, int64_t pz, Cell& c) {
   const int64_t idx = p[0] + D.n[0] * (p[1] + D.n[1] * p[2]);
   const Lattice& L = *D.L;
   for (int i = 0; i < L.Q; i++) c.f[i] = D.f[(int64_t)i * D.N + idx];
+  if (D.h) for (int i = 0; i < L.Q; i++) c.h[i] = D.h[(int64_t)i * D.N + idx];
   c.rho = D.rho[idx];
   for (int k = 0; k < 4; k++) c.uT[k] = D.g[(int64_t)k * D.N + idx];
   for (int a = 0; a < 3; a++) {
@@ -336,12 +363,16 @@ void load_cell(const Domain& D, int64_t px, int64_t py, int64_t pz, Cell& c) {
     double fn[QMAX];
     for (int i = 0; i < L.Q; i++) fn[i] = (L.e[i][a] == 0) ? c.f[i] : c.f[L.rev[a][i]];
     for (int i = 0; i < L.Q; i++) c.f[i] = fn[i];
+    if (D.h) {
+      for (int i = 0; i < L.Q; i++) fn[i] = (L.e[i][a] == 0) ? c.h[i] : c.h[L.rev[a][i]];
+      for (int i = 0; i < L.Q; i++) c.h[i] = fn[i];
+    }
   }
 }
 
 // steps.cu:986-1036 propagate<N> (N = 2..5) -- Lagrange interpolation of the
 // gauge-transformed stencil at the departure point crd.
-double propagate(const Domain& D, int N, const double crd[3], int i, const double* base) {
+double propagate(const Domain& D, int N, const double crd[3], int i, const double* base, bool energy = false) {
   int64_t cl[3];
   if (N % 2 == 0) {
     for (int a = 0; a < 3; a++) cl[a] = (int64_t)(std::floor(crd[a]) - N / 2 + 1);
@@ -361,13 +392,14 @@ double propagate(const Domain& D, int N, const double crd[3], int i, const doubl
         // NaN for every stencil cell alike), so skipping it is exact
         if (a == 0) continue;
         load_cell(D, cl[0] + ix, cl[1] + iy, cl[2] + iz, c);
-        fpr += a * transfer_gauge(*D.L, c, base, i);
+        fpr += a * transfer_gauge(*D.L, c, base, i, energy);
       }
   return fpr;
 }
 
 // steps.cu:924-937 LagrEval<N> (explicit stencil origin)
-double lagr_eval(const Domain& D, int N, const double crd[3], const int64_t cl[3], int i, const double* base) {
+double lagr_eval(const Domain& D, int N, const double crd[3], const int64_t cl[3], int i, const double* base,
+                 bool energy = false) {
   const double sx = crd[0] - cl[0], sy = crd[1] - cl[1], sz = crd[2] - cl[2];
   double fpr = 0;
   Cell c;
@@ -377,20 +409,20 @@ double lagr_eval(const Domain& D, int N, const double crd[3], const int64_t cl[3
         const double a = (N == 2) ? lin_pol(ix, iy, iz, sx, sy, sz) : lagr_pol(N, ix, iy, iz, sx, sy, sz);
         if (a == 0) continue;
         load_cell(D, cl[0] + ix, cl[1] + iy, cl[2] + iz, c);
-        fpr += a * transfer_gauge(*D.L, c, base, i);
+        fpr += a * transfer_gauge(*D.L, c, base, i, energy);
       }
   return fpr;
 }
 
 // steps.cu:774-825 propagateWENO<3,5>
-double propagate_weno5(const Domain& D, const double crd[3], int i, const double* base) {
+double propagate_weno5(const Domain& D, const double crd[3], int i, const double* base, bool energy = false) {
   const double fx = std::floor(crd[0] + 0.5), fy = std::floor(crd[1] + 0.5), fz = std::floor(crd[2] + 0.5);
   const int64_t c0[3] = {(int64_t)(fx - 2), (int64_t)fy, (int64_t)fz};
   const int64_t c1[3] = {(int64_t)(fx - 1), (int64_t)fy, (int64_t)fz};
   const int64_t c2[3] = {(int64_t)(fx), (int64_t)fy, (int64_t)fz};
-  const double S0 = lagr_eval(D, 3, crd, c0, i, base);
-  const double S1 = lagr_eval(D, 3, crd, c1, i, base);
-  const double S2 = lagr_eval(D, 3, crd, c2, i, base);
+  const double S0 = lagr_eval(D, 3, crd, c0, i, base, energy);
+  const double S1 = lagr_eval(D, 3, crd, c1, i, base, energy);
+  const double S2 = lagr_eval(D, 3, crd, c2, i, base, energy);
   const double cdist = crd[0] - (int)(std::floor(crd[0] + 0.5));
   const double d0 = (cdist * cdist - 3 * cdist + 2) / 12.;
   const double d2 = (cdist * cdist + 3 * cdist + 2) / 12.;
@@ -401,7 +433,7 @@ double propagate_weno5(const Domain& D, const double crd[3], int i, const double
   Cell c;
   for (int k = 1; k <= 5; k++) {
     load_cell(D, lx + (k - 1), ly, lz, c);
-    u[k] = transfer_gauge(*D.L, c, base, i);
+    u[k] = transfer_gauge(*D.L, c, base, i, energy);
   }
   const double u1 = u[1], u2 = u[2], u3 = u[3], u4 = u[4], u5 = u[5];
   const double beta0 = (10 * u3 * u3 + (11 * u1 - 31 * u2) * u3 + 25 * u2 * u2 - 19 * u1 * u2 + 4 * u1 * u1) / 3.0;
@@ -426,7 +458,8 @@ double minmod(double a, double b) {
 
 // steps.cu:447 with FluxTVDdif (:118-124): plain cubic value at x-v plus a
 // minmod-limited flux-difference correction
-double propagate_tvd(const Domain& D, const double coord[3], const double v[3], int i, const double* base) {
+double propagate_tvd(const Domain& D, const double coord[3], const double v[3], int i, const double* base,
+                     bool energy = false) {
   double cM2[3], cM1[3], cC[3], cP1[3];
   for (int a = 0; a < 3; a++) {
     cM2[a] = coord[a] - v[a] * 2;
@@ -434,27 +467,36 @@ double propagate_tvd(const Domain& D, const double coord[3], const double v[3], 
     cC[a] = coord[a] + v[a] * 0;
     cP1[a] = coord[a] + v[a] * 1;
   }
-  const double Fm1 = propagate(D, 4, cM1, i, base);
-  const double Fm2 = propagate(D, 4, cM2, i, base);
-  const double F0 = propagate(D, 4, cC, i, base);
-  const double Fp1 = propagate(D, 4, cP1, i, base);
+  const double Fm1 = propagate(D, 4, cM1, i, base, energy);
+  const double Fm2 = propagate(D, 4, cM2, i, base, energy);
+  const double F0 = propagate(D, 4, cC, i, base, energy);
+  const double Fp1 = propagate(D, 4, cP1, i, base, energy);
   const int sg = sign_i(v[0]);
   const double flux = F0 - Fm1 + sg * 0.5 * minmod(F0 - Fm1, Fp1 - F0) - sg * 0.5 * minmod(F0 - Fm1, Fm1 - Fm2);
-  const double fc = propagate(D, 4, coord, i, base);
+  const double fc = propagate(D, 4, coord, i, base, energy);
   return fc - flux;
 }
 
 // steps.cu:356-588 LBMpull (and :151-250 PonDstepD3Q125 for FIXED3): the
 // fixed-point gauge iteration, BGK relaxation and store for one node.
+//
+// With the double-distribution extension (D.h set), the energy populations h
+// are transferred and interpolated exactly as f, the temperature of each
+// iterate comes from their sum, T = (sum h / rho - |u|^2) / (Dim + dof), the
+// convergence test covers them too, and they relax to the equilibrium of
+// set_energy.  The model's heat-capacity ratio is (Dim + dof + 2)/(Dim + dof).
 int pull_node(const Domain& D, const orc_params& P, int64_t x, int64_t y, int64_t z,
-              const double* guess, double* f_out, double* rho_out, double* g_out, int* niter_out) {
+              const double* guess, double* f_out, double* h_out, double* rho_out, double* g_out, int* niter_out) {
   const Lattice& L = *D.L;
+  const bool ddf = D.h != nullptr;
+  const double dof = P.dof;
   const int64_t idx = x + D.n[0] * (y + D.n[1] * z);
   Cell c0, cnew;
   load_cell(D, x, y, z, c0);
   if (c0.rho == 0 && c0.uT[0] == 0 && c0.uT[1] == 0 && c0.uT[2] == 0 && c0.uT[3] == 0) {
     const double b[4] = {0, 0, 0, L.TLat};
     set_base(L, c0, 1, b);
+    if (ddf) set_energy(L, c0, dof);
   }
   if (guess) for (int k = 0; k < 4; k++) c0.uT[k] = guess[(int64_t)k * D.N + idx];
   const double coord[3] = {(double)x, (double)y, (double)z};
@@ -480,31 +522,56 @@ int pull_node(const Domain& D, const orc_params& P, int64_t x, int64_t y, int64_
       double val = 0;
       switch (P.interp) {
         case ORC_FIXED3: {
-          double newval[27];
-          for (int k = 0; k < 27; k++) newval[k] = transfer_gauge(L, cfix[k], uT, i);
-          const double sx = crd[0] - (x - 1), sy = crd[1] - (y - 1), sz = crd[2] - (z - 1);
-          double fpr = 0;
-          for (int a = 0; a < 3; a++)
-            for (int b = 0; b < 3; b++)
-              for (int c = 0; c < 3; c++) fpr += lagr_pol(3, a, b, c, sx, sy, sz) * newval[9 * a + 3 * b + c];
-          val = fpr;
+          for (int e = 0; e < (ddf ? 2 : 1); e++) {
+            double newval[27];
+            for (int k = 0; k < 27; k++) newval[k] = transfer_gauge(L, cfix[k], uT, i, e == 1);
+            const double sx = crd[0] - (x - 1), sy = crd[1] - (y - 1), sz = crd[2] - (z - 1);
+            double fpr = 0;
+            for (int a = 0; a < 3; a++)
+              for (int b = 0; b < 3; b++)
+                for (int c = 0; c < 3; c++) fpr += lagr_pol(3, a, b, c, sx, sy, sz) * newval[9 * a + 3 * b + c];
+            if (e == 0) val = fpr; else cnew.h[i] = fpr;
+          }
           break;
         }
-        case ORC_TVD: val = propagate_tvd(D, coord, vi[i], i, uT); break;
-        case ORC_WENO5: val = propagate_weno5(D, crd, i, uT); break;
-        default: val = propagate(D, P.interp, crd, i, uT); break;
+        case ORC_TVD:
+          val = propagate_tvd(D, coord, vi[i], i, uT);
+          if (ddf) cnew.h[i] = propagate_tvd(D, coord, vi[i], i, uT, true);
+          break;
+        case ORC_WENO5:
+          val = propagate_weno5(D, crd, i, uT);
+          if (ddf) cnew.h[i] = propagate_weno5(D, crd, i, uT, true);
+          break;
+        default:
+          val = propagate(D, P.interp, crd, i, uT);
+          if (ddf) cnew.h[i] = propagate(D, P.interp, crd, i, uT, true);
+          break;
       }
       cnew.f[i] = val;
     }
     calc_moments(L, cnew, vi);
+    if (ddf) {  // the temperature of the iterate from its energy populations
+      double e = 0;
+      for (int i = 0; i < L.Q; i++) e += cnew.h[i];
+      if (cnew.rho != 0) e /= cnew.rho;
+      cnew.uT[3] = (e - cnew.uT[0] * cnew.uT[0] - cnew.uT[1] * cnew.uT[1] - cnew.uT[2] * cnew.uT[2]) / (L.Dim + dof);
+    }
     if (cnew.uT[3] < 0) cnew.uT[3] = c0.uT[3];  // steps.cu:475-478
-    if (is_conv(L, cnew, c0, P.tol_abs, P.tol_rel)) { c0 = cnew; conv = true; break; }
+    if (is_conv(L, cnew, c0, P.tol_abs, P.tol_rel, ddf)) { c0 = cnew; conv = true; break; }
     c0 = cnew;
   }
   const double dtau = 1.0 / P.tau;
   for (int i = 0; i < L.Q; i++) {  // steps.cu:557-564
     const double feq = c0.rho * L.w[i];
     c0.f[i] += dtau * (feq - c0.f[i]);
+  }
+  if (ddf) {
+    Cell eq = c0;
+    set_energy(L, eq, dof);
+    for (int i = 0; i < L.Q; i++) {
+      c0.h[i] += dtau * (eq.h[i] - c0.h[i]);
+      h_out[(int64_t)i * D.N + idx] = c0.h[i];
+    }
   }
   for (int i = 0; i < L.Q; i++) f_out[(int64_t)i * D.N + idx] = c0.f[i];
   rho_out[idx] = c0.rho;
@@ -573,13 +640,29 @@ double orc_lagr_pol(int n, int ix, int iy, int iz, double sx, double sy, double 
   return n == 2 ? lin_pol(ix, iy, iz, sx, sy, sz) : lagr_pol(n, ix, iy, iz, sx, sy, sz);
 }
 
+void orc_set_energy(int lattice_kind, double rho, const double* uT, double dof, double* h) {
+  const Lattice& L = lattice(lattice_kind);
+  Cell c;
+  c.rho = rho;
+  for (int k = 0; k < 4; k++) c.uT[k] = uT[k];
+  set_energy(L, c, dof);
+  for (int i = 0; i < L.Q; i++) h[i] = c.h[i];
+}
+
 int64_t orc_step(const orc_params* p, const double* f_in, const double* rho_in, const double* g_in,
                  const double* guess, double* f_out, double* rho_out, double* g_out, int* niter) {
+  return orc_step_ddf(p, f_in, nullptr, rho_in, g_in, guess, f_out, nullptr, rho_out, g_out, niter);
+}
+
+int64_t orc_step_ddf(const orc_params* p, const double* f_in, const double* h_in, const double* rho_in,
+                     const double* g_in, const double* guess, double* f_out, double* h_out, double* rho_out,
+                     double* g_out, int* niter) {
   const Lattice& L = lattice(p->lattice);
   if (L.Q == 0 || p->nx <= 0 || p->ny <= 0 || p->nz <= 0 || p->max_iter <= 0) return -1;
+  if ((h_in == nullptr) != (h_out == nullptr) || (h_in && !(p->dof >= 0))) return -1;
   Domain D;
   D.L = &L;
-  D.f = f_in; D.rho = rho_in; D.g = g_in;
+  D.f = f_in; D.h = h_in; D.rho = rho_in; D.g = g_in;
   D.n[0] = p->nx; D.n[1] = p->ny; D.n[2] = p->nz;
   D.N = p->nx * p->ny * p->nz;
   for (int a = 0; a < 3; a++) D.bc[a] = p->bc[a];
@@ -592,7 +675,7 @@ int64_t orc_step(const orc_params* p, const double* f_in, const double* rho_in, 
 #endif
   for (int64_t n = 0; n < N; n++) {
     const int64_t x = n % p->nx, y = (n / p->nx) % p->ny, z = n / (p->nx * p->ny);
-    nonconv += pull_node(D, P, x, y, z, guess, f_out, rho_out, g_out, niter);
+    nonconv += pull_node(D, P, x, y, z, guess, f_out, h_out, rho_out, g_out, niter);
   }
   return nonconv;
 }

@@ -38,6 +38,7 @@ typedef struct {
   double tol_rel;     /* isConv relative tolerance (steps.cu:63) */
   int max_iter;       /* iteration cap (steps.cu:422) */
   int nthreads;       /* 0 = OpenMP default */
+  double dof;         /* double-distribution extension: extra degrees of freedom (orc_step_ddf) */
 } orc_params;
 
 int    orc_q(int lattice);
@@ -59,6 +60,14 @@ int64_t orc_step(const orc_params* p,
                  const double* f_in, const double* rho_in, const double* g_in,
                  const double* guess,
                  double* f_out, double* rho_out, double* g_out, int* niter);
+/* Double-distribution extension (energy populations h, same layout as f):
+   gamma = (Dim + dof + 2) / (Dim + dof).  orc_set_energy gives the
+   equilibrium h of one node; orc_step_ddf is orc_step carrying h. */
+void   orc_set_energy(int lattice, double rho, const double* uT, double dof, double* h);
+int64_t orc_step_ddf(const orc_params* p,
+                     const double* f_in, const double* h_in, const double* rho_in, const double* g_in,
+                     const double* guess,
+                     double* f_out, double* h_out, double* rho_out, double* g_out, int* niter);
 int    orc_max_threads(void);
 
 #ifdef __cplusplus
