@@ -84,7 +84,12 @@ typedef struct {
   int max_iter;    /* fixed-point iteration cap (steps.cu:422: 100) */
   int device;      /* CUDA device ordinal */
   int learned;     /* 1: start each node's iteration from the predictor's gauge */
-  int reserved[5];
+  int ddf;         /* 1: energy populations (double-distribution extension, D1Q5): a second
+                      population set carries the total energy, gamma = (Dim+dof+2)/(Dim+dof);
+                      completes the reference's DDF scaffolding (structs.cuh:37-39,336-341,391-394,
+                      lbpack.cu:18-20, steps.cu:233-236) */
+  int ddf_dof;     /* extra degrees of freedom dof >= 0 of the extension (4: gamma = 1.4 in 1D) */
+  int reserved[3];
 } pond_params;
 
 /* diagnostics of the last completed step (update.cu:124-135, diagn.cu:24-30) */
@@ -119,9 +124,16 @@ int pond_q(int lattice);
    SPHERE {cx, cy, cz, radius, rho_in, T_in, rho_out, T_out};
    TGV {U0, T0, rho0, gamma}; UNIFORM {rho, ux, uy, uz, T} */
 int pond_init(pond_ctx* ctx, int ic, const double* ic_params, int n_params);
-/* upload a state from host memory; f == NULL applies set_base (f_i = w_i*rho) */
+/* upload a state from host memory; f == NULL applies set_base (f_i = w_i*rho);
+   a context with energy populations (ddf = 1) also gets them at equilibrium,
+   h_i = rho w_i (|v_i|^2 + ddf_dof T) */
 int pond_set_state(pond_ctx* ctx, const double* f, const double* rho, const double* g);
 int pond_get_state(pond_ctx* ctx, double* f, double* rho, double* g);
+/* energy populations h[Q*N] (reference population order) of a ddf = 1 context:
+   the reference's Cell::h (structs.cuh:37-39), which its scaffolding never
+   initialises or stores; set after pond_set_state / pond_init */
+int pond_set_energy(pond_ctx* ctx, const double* h);
+int pond_get_energy(pond_ctx* ctx, double* h);
 /* any pointer may be NULL; each receives N values */
 int pond_get_fields(pond_ctx* ctx, double* rho, double* ux, double* uy, double* uz, double* T);
 /* advance nsteps steps (calcStep without drop/diagnostics printing) */

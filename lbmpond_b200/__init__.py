@@ -48,7 +48,9 @@ class Solver:
 
     def __init__(self, lattice="D3Q27", shape=(32, 32, 32), interp=None, precision="fp32", tau=0.9,
                  tol_abs=None, tol_rel=None, max_iter=100, bc=("periodic",) * 3, device=0, dt=1.0,
-                 learned=False):
+                 learned=False, ddf_dof=None):
+        """``ddf_dof``: carry energy populations with that many extra degrees
+        of freedom (D1Q5 1D grids; gamma = (Dim + dof + 2) / (Dim + dof))."""
         L = _lib.load()
         lat = _LATTICES.get(lattice, lattice)
         p = _lib.PondParams()
@@ -68,6 +70,8 @@ class Solver:
         p.max_iter = max_iter
         p.device = device
         p.learned = 1 if learned else 0
+        if ddf_dof is not None:
+            p.ddf, p.ddf_dof = 1, int(ddf_dof)
         for a in range(3):
             p.bc[a] = _BCS.get(bc[a], bc[a])
         ctx = ctypes.c_void_p()
@@ -120,6 +124,16 @@ class Solver:
         f = np.empty((self.Q, self.N)); rho = np.empty(self.N); g = np.empty((4, self.N))
         _lib.check(self._L.pond_get_state(self._ctx, _dp(f), _dp(rho), _dp(g)))
         return f, rho, g
+
+    def set_energy(self, h):
+        """Energy populations h[Q, N] of a context made with ``ddf_dof``."""
+        h = np.ascontiguousarray(h, dtype=np.float64).reshape(self.Q, self.N)
+        _lib.check(self._L.pond_set_energy(self._ctx, _dp(h)))
+
+    def get_energy(self):
+        h = np.empty((self.Q, self.N))
+        _lib.check(self._L.pond_get_energy(self._ctx, _dp(h)))
+        return h
 
     def fields(self):
         out = [np.empty(self.N) for _ in range(5)]

@@ -28,7 +28,8 @@ class PondParams(ctypes.Structure):
         ("tau", ctypes.c_double), ("dt", ctypes.c_double),
         ("tol_abs", ctypes.c_double), ("tol_rel", ctypes.c_double),
         ("max_iter", ctypes.c_int), ("device", ctypes.c_int), ("learned", ctypes.c_int),
-        ("reserved", ctypes.c_int * 5),
+        ("ddf", ctypes.c_int), ("ddf_dof", ctypes.c_int),
+        ("reserved", ctypes.c_int * 3),
     ]
 
 
@@ -57,6 +58,8 @@ SIGNATURES = {
     "pond_init": (ctypes.c_int, [_vp, ctypes.c_int, _dp, ctypes.c_int]),
     "pond_set_state": (ctypes.c_int, [_vp, _dp, _dp, _dp]),
     "pond_get_state": (ctypes.c_int, [_vp, _dp, _dp, _dp]),
+    "pond_set_energy": (ctypes.c_int, [_vp, _dp]),
+    "pond_get_energy": (ctypes.c_int, [_vp, _dp]),
     "pond_get_fields": (ctypes.c_int, [_vp, _dp, _dp, _dp, _dp, _dp]),
     "pond_step": (ctypes.c_int, [_vp, ctypes.c_int]),
     "pond_diagnostics": (ctypes.c_int, [_vp, ctypes.POINTER(PondDiag)]),

@@ -78,11 +78,12 @@ struct FillArgs {
   long long N;
   int Q;
   double dim;
+  double dof;  // extra degrees of freedom of the energy populations
   double w[125];
 };
 
 template <typename R>
-__global__ void fill_kernel(FillArgs a, R* f0, R* rho0, R* g0, R* f1, R* rho1, R* g1) {
+__global__ void fill_kernel(FillArgs a, R* f0, R* rho0, R* g0, R* f1, R* rho1, R* g1, R* h0, R* h1) {
   const long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n >= a.N) return;
   const int x = n % a.nx, y = (n / a.nx) % a.ny, z = n / ((long long)a.nx * a.ny);
@@ -137,6 +138,12 @@ __global__ void fill_kernel(FillArgs a, R* f0, R* rho0, R* g0, R* f1, R* rho1, R
   rho0[n] = R(rho); rho1[n] = R(rho);
   const R gv[4] = {R(ux), R(uy), R(uz), R(T)};
   for (int k = 0; k < 4; k++) { g0[k * a.N + n] = gv[k]; g1[k * a.N + n] = gv[k]; }
+  if (h0) {  // equilibrium energy populations (D1Q5)
+    const double U[3] = {ux, uy, uz};
+    R h[5];
+    energy_equilibrium<R>(rho, U, T, a.dof, h);
+    for (int q = 0; q < 5; q++) { h0[(long long)q * a.N + n] = h[q]; h1[(long long)q * a.N + n] = h[q]; }
+  }
 }
 
 }  // namespace pond
@@ -204,6 +211,13 @@ int pond_create(const pond_params* p, pond_ctx** out) {
   if (!(p->tol_abs >= 0) || !(p->tol_rel >= 0)) return set_error(POND_ERR_ARG, "tolerances must be >= 0");
   if (p->lattice == POND_D1Q5 && (p->interp == POND_TVD || p->interp == POND_WENO5) && (p->Ny != 1 || p->Nz != 1))
     return set_error(POND_ERR_UNSUPPORTED, "TVD/WENO5 run on 1D grids (Ny = Nz = 1)");
+  if (p->ddf != 0 && p->ddf != 1) return set_error(POND_ERR_ARG, "ddf must be 0 or 1");
+  if (p->ddf) {
+    if (p->lattice != POND_D1Q5 || p->Ny != 1 || p->Nz != 1)
+      return set_error(POND_ERR_UNSUPPORTED, "energy populations run on D1Q5 1D grids");
+    if (p->ddf_dof < 0 || p->ddf_dof > 1000) return set_error(POND_ERR_ARG, "ddf_dof must be in 0..1000");
+    if (p->learned) return set_error(POND_ERR_UNSUPPORTED, "the learned start does not carry energy populations");
+  }
 
   int ndev = 0;
   cudaError_t e = cudaGetDeviceCount(&ndev);
@@ -275,16 +289,19 @@ int pond_init(pond_ctx* c, int ic, const double* prm, int nprm) {
   a.N = c->N;
   a.Q = c->Q;
   a.dim = dim;
+  a.dof = c->p.ddf_dof;
   for (int q = 0; q < c->Q; q++) a.w[q] = lattice_weight_host(c->p.lattice, q);
   const int th = 256;
   const unsigned blocks = (unsigned)((c->N + th - 1) / th);
   const int o = c->cur, n = 1 - c->cur;
   if (c->elem == 8)
     fill_kernel<double><<<blocks, th, 0, c->stream>>>(a, (double*)c->f[o], (double*)c->rho[o], (double*)c->g[o],
-                                                       (double*)c->f[n], (double*)c->rho[n], (double*)c->g[n]);
+                                                       (double*)c->f[n], (double*)c->rho[n], (double*)c->g[n],
+                                                       (double*)c->h[o], (double*)c->h[n]);
   else
     fill_kernel<float><<<blocks, th, 0, c->stream>>>(a, (float*)c->f[o], (float*)c->rho[o], (float*)c->g[o],
-                                                      (float*)c->f[n], (float*)c->rho[n], (float*)c->g[n]);
+                                                      (float*)c->f[n], (float*)c->rho[n], (float*)c->g[n],
+                                                      (float*)c->h[o], (float*)c->h[n]);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "fill kernel launch");
   e = cudaStreamSynchronize(c->stream);
@@ -314,12 +331,23 @@ int pond_set_state(pond_ctx* c, const double* f, const double* rho, const double
   int st = upload(c, f, (size_t)Q * N, c->f[c->cur]);
   if (st == POND_OK) st = upload(c, rho, (size_t)N, c->rho[c->cur]);
   if (st == POND_OK) st = upload(c, g, (size_t)4 * N, c->g[c->cur]);
+  if (st == POND_OK && c->p.ddf) {  // energy populations at equilibrium in every node's gauge
+    std::vector<double> hb((size_t)Q * N);
+    for (long long n = 0; n < N; n++) {
+      const double U[3] = {g[n], g[N + n], g[2 * N + n]};
+      double h[5];
+      energy_equilibrium<double>(rho[n], U, g[3 * N + n], c->p.ddf_dof, h);
+      for (int q = 0; q < Q; q++) hb[(size_t)q * N + n] = h[q];
+    }
+    st = upload(c, hb.data(), (size_t)Q * N, c->h[c->cur]);
+  }
   if (st != POND_OK) return st;
   // the reference fills both buffers (init.cu:104-105)
-  const size_t bytes[3] = {(size_t)Q * N * c->elem, (size_t)N * c->elem, (size_t)4 * N * c->elem};
-  void* src[3] = {c->f[c->cur], c->rho[c->cur], c->g[c->cur]};
-  void* dst[3] = {c->f[1 - c->cur], c->rho[1 - c->cur], c->g[1 - c->cur]};
-  for (int k = 0; k < 3; k++) {
+  const size_t bytes[4] = {(size_t)Q * N * c->elem, (size_t)N * c->elem, (size_t)4 * N * c->elem,
+                           (size_t)Q * N * c->elem};
+  void* src[4] = {c->f[c->cur], c->rho[c->cur], c->g[c->cur], c->h[c->cur]};
+  void* dst[4] = {c->f[1 - c->cur], c->rho[1 - c->cur], c->g[1 - c->cur], c->h[1 - c->cur]};
+  for (int k = 0; k < (c->p.ddf ? 4 : 3); k++) {
     cudaError_t e = cudaMemcpyAsync(dst[k], src[k], bytes[k], cudaMemcpyDeviceToDevice, c->stream);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync D2D");
   }
@@ -340,6 +368,29 @@ int pond_get_state(pond_ctx* c, double* f, double* rho, double* g) {
   if (st == POND_OK && rho) st = download(c, c->rho[c->cur], (size_t)c->N, rho);
   if (st == POND_OK && g) st = download(c, c->g[c->cur], (size_t)4 * c->N, g);
   return st;
+}
+
+int pond_set_energy(pond_ctx* c, const double* h) {
+  if (!c || !h) return set_error(POND_ERR_ARG, "pond_set_energy: null argument");
+  if (!c->p.ddf) return set_error(POND_ERR_STATE, "the context has no energy populations (ddf = 0)");
+  { const int ps = pipe_drain(c); if (ps != POND_OK) return ps; }
+  if (!c->initialized) return set_error(POND_ERR_STATE, "set the state before its energy populations");
+  cudaSetDevice(c->p.device);
+  const size_t cnt = (size_t)c->Q * c->N;
+  int st = upload(c, h, cnt, c->h[c->cur]);
+  if (st != POND_OK) return st;
+  cudaError_t e = cudaMemcpyAsync(c->h[1 - c->cur], c->h[c->cur], cnt * c->elem, cudaMemcpyDeviceToDevice, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  return e == cudaSuccess ? POND_OK : cuda_fail(e, "pond_set_energy");
+}
+
+int pond_get_energy(pond_ctx* c, double* h) {
+  if (!c || !h) return set_error(POND_ERR_ARG, "pond_get_energy: null argument");
+  if (!c->p.ddf) return set_error(POND_ERR_STATE, "the context has no energy populations (ddf = 0)");
+  { const int ps = pipe_drain(c); if (ps != POND_OK) return ps; }
+  if (!c->initialized) return set_error(POND_ERR_STATE, "state not initialised");
+  cudaSetDevice(c->p.device);
+  return download(c, c->h[c->cur], (size_t)c->Q * c->N, h);
 }
 
 int pond_get_fields(pond_ctx* c, double* rho, double* ux, double* uy, double* uz, double* T) {
@@ -431,6 +482,7 @@ int pond_last_step_ms(pond_ctx* c, float* ms) {
 
 int pond_upload_state(pond_ctx* c, const void* f, const void* rho, const void* g) {
   if (!c || !f || !rho || !g) return set_error(POND_ERR_ARG, "pond_upload_state: null argument");
+  if (c->p.ddf) return set_error(POND_ERR_UNSUPPORTED, "pond_upload_state carries no energy populations");
   { const int ps = pipe_drain(c); if (ps != POND_OK) return ps; }
   cudaSetDevice(c->p.device);
   const size_t N = (size_t)c->N;
@@ -475,16 +527,17 @@ int pond_copy_state(pond_ctx* dst, pond_ctx* src) {
   if (dst->p.lattice != src->p.lattice || dst->N != src->N || dst->p.Nx != src->p.Nx || dst->p.Ny != src->p.Ny)
     return set_error(POND_ERR_ARG, "pond_copy_state: lattice or grid differ");
   if (dst->p.device != src->p.device) return set_error(POND_ERR_ARG, "pond_copy_state: contexts on different devices");
+  if (dst->p.ddf != src->p.ddf) return set_error(POND_ERR_ARG, "pond_copy_state: one context has energy populations");
   if (!src->initialized) return set_error(POND_ERR_STATE, "source state not initialised");
   cudaSetDevice(dst->p.device);
   cudaError_t e = cudaStreamSynchronize(src->stream);
   if (e != cudaSuccess) return cuda_fail(e, "pond_copy_state");
-  const long long cnt[3] = {(long long)dst->Q * dst->N, dst->N, 4 * dst->N};
+  const long long cnt[4] = {(long long)dst->Q * dst->N, dst->N, 4 * dst->N, (long long)dst->Q * dst->N};
   for (int b = 0; b < 2; b++) {  // both time levels: the current one and the one before it
     const int sb = b == 0 ? src->cur : 1 - src->cur, db = b == 0 ? dst->cur : 1 - dst->cur;
-    void* d[3] = {dst->f[db], dst->rho[db], dst->g[db]};
-    const void* s3[3] = {src->f[sb], src->rho[sb], src->g[sb]};
-    for (int k = 0; k < 3; k++) {
+    void* d[4] = {dst->f[db], dst->rho[db], dst->g[db], dst->h[db]};
+    const void* s3[4] = {src->f[sb], src->rho[sb], src->g[sb], src->h[sb]};
+    for (int k = 0; k < (dst->p.ddf ? 4 : 3); k++) {
       if (dst->elem == src->elem) {
         e = cudaMemcpyAsync(d[k], s3[k], cnt[k] * dst->elem, cudaMemcpyDeviceToDevice, dst->stream);
       } else if (dst->elem == 8) {

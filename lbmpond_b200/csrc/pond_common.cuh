@@ -141,6 +141,21 @@ struct StepSums {
 };
 
 // Arguments of the step kernels.
+// Equilibrium energy populations of one D1Q5 node in the gauge (U, T) for
+// the double-distribution extension: h_i = rho w_i (|v_i|^2 + dof T),
+// v_i = U + sqrt(T/TLat) xi_i (population order = class order for D1Q5).
+template <typename R>
+__host__ __device__ inline void energy_equilibrium(double rho, const double U[3], double T, double dof, R h[5]) {
+  using L = Lattice<POND_D1Q5>;
+  const double C = sqrt(fabs(T) * (1.0 / L::TLat));
+  const double side = U[1] * U[1] + U[2] * U[2];
+#pragma unroll
+  for (int k = 0; k < 5; k++) {
+    const double vx = C * L::xi1(k) + U[0];
+    h[k] = R(rho * lattice_weight_t<POND_D1Q5>(k) * (vx * vx + side + dof * T));
+  }
+}
+
 template <typename R> struct StepArgs {
   const R* f_in;   // [Q][N]
   const R* rho_in; // [N]
@@ -158,6 +173,10 @@ template <typename R> struct StepArgs {
   double tol_abs, tol_rel;
   int max_iter;
   double kdx;  // 0.5 * dx*dy*dz / (8 pi^3) with dx = 2 pi / Nx (diagn.cu:14-18)
+  // energy populations of the double-distribution extension (D1Q5), or null
+  const R* h_in = nullptr;  // [Q][N]
+  R* h_out = nullptr;
+  double dof = 0;           // extra degrees of freedom
 };
 
 }  // namespace pond

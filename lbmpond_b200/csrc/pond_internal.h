@@ -15,6 +15,7 @@ struct pond_ctx {
   void* f[2] = {nullptr, nullptr};
   void* rho[2] = {nullptr, nullptr};
   void* g[2] = {nullptr, nullptr};
+  void* h[2] = {nullptr, nullptr};  // energy populations h[Q][N] (double-distribution extension)
   int cur = 0;
   pond::StepSums* d_sums = nullptr;
   pond::StepSums* h_sums = nullptr;  // pinned

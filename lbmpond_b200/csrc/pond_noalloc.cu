@@ -115,6 +115,7 @@ extern "C" int pond_step_noalloc(const pond_params* p, const float* f_in, const 
     return set_error(POND_ERR_ARG, "pond_step_noalloc: null argument");
   if (p->lattice != POND_D3Q27 || p->precision != POND_FP32 || p->interp < POND_LAGR2 || p->interp > POND_LAGR4)
     return set_error(POND_ERR_UNSUPPORTED, "pond_step_noalloc runs D3Q27, float32, Lagrange order 2-4 only");
+  if (p->ddf) return set_error(POND_ERR_UNSUPPORTED, "pond_step_noalloc carries no energy populations");
   if (p->Nx <= 0 || p->Ny <= 0 || p->Nz <= 0 || p->Nx > (1 << 30) || p->Ny > (1 << 30) || p->Nz > (1 << 30))
     return set_error(POND_ERR_ARG, "grid out of range");
   const long long N = p->Nx * p->Ny * p->Nz;

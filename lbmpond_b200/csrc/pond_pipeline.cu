@@ -76,6 +76,7 @@ int pond_step_host(pond_ctx* c, const void* f_in, const void* rho_in, const void
   if (!c || !f_in || !rho_in || !g_in) return set_error(POND_ERR_ARG, "pond_step_host: null input");
   if (!c->initialized) return set_error(POND_ERR_STATE, "pond_step_host before pond_init/pond_set_state");
   if (c->p.learned) return set_error(POND_ERR_STATE, "pond_step_host runs the plain start; detach the predictor");
+  if (c->p.ddf) return set_error(POND_ERR_UNSUPPORTED, "pond_step_host carries no energy populations");
   cudaSetDevice(c->p.device);
   int st = pipe_setup(c);
   if (st != POND_OK) return st;

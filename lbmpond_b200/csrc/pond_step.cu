@@ -7,6 +7,7 @@
 
 #include "pond_internal.h"
 #include "pond_step_1d.cuh"
+#include "pond_step_1d_energy.cuh"
 #include "pond_step_d3q125.cuh"
 #include "pond_step_d3q125_tile.cuh"
 #include "pond_step_d3q27.cuh"
@@ -22,9 +23,11 @@ int ctx_alloc(pond_ctx* c) {
   const size_t N = (size_t)c->N;
   for (int b = 0; b < 2; b++) {
     if (cudaMalloc(&c->f[b], (size_t)c->Q * N * c->elem) != cudaSuccess ||
-        cudaMalloc(&c->rho[b], N * c->elem) != cudaSuccess || cudaMalloc(&c->g[b], 4 * N * c->elem) != cudaSuccess) {
+        cudaMalloc(&c->rho[b], N * c->elem) != cudaSuccess || cudaMalloc(&c->g[b], 4 * N * c->elem) != cudaSuccess ||
+        (c->p.ddf && cudaMalloc(&c->h[b], (size_t)c->Q * N * c->elem) != cudaSuccess)) {
       cudaGetLastError();
-      return set_error(POND_ERR_NOMEM, "state buffers (%zu bytes each)", (size_t)(c->Q + 5) * N * c->elem);
+      return set_error(POND_ERR_NOMEM, "state buffers (%zu bytes each)",
+                       (size_t)(c->Q * (c->p.ddf ? 2 : 1) + 5) * N * c->elem);
     }
   }
   if (cudaMalloc(&c->d_sums, sizeof(StepSums)) != cudaSuccess) {
@@ -40,8 +43,8 @@ void ctx_free(pond_ctx* c) {
   pipe_free(c);
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (int b = 0; b < 2; b++) {
-    cudaFree(c->f[b]); cudaFree(c->rho[b]); cudaFree(c->g[b]);
-    c->f[b] = c->rho[b] = c->g[b] = nullptr;
+    cudaFree(c->f[b]); cudaFree(c->rho[b]); cudaFree(c->g[b]); cudaFree(c->h[b]);
+    c->f[b] = c->rho[b] = c->g[b] = c->h[b] = nullptr;
   }
   cudaFree(c->d_sums); c->d_sums = nullptr;
   cudaFree(c->niter); c->niter = nullptr;
@@ -134,7 +137,7 @@ int state_sums(pond_ctx* c, pond_diag* out) {
   if (e != cudaSuccess) return cuda_fail(e, "memset");
   const int th = 256;
   const unsigned blocks = (unsigned)((c->N + th - 1) / th);
-  const double dim = lattice_dim(c->p.lattice);
+  const double dim = lattice_dim(c->p.lattice) + (c->p.ddf ? c->p.ddf_dof : 0);  // total energy's degrees
   if (c->elem == 8)
     state_sums_kernel<double><<<blocks, th, 0, c->stream>>>((const double*)c->rho[c->cur], (const double*)c->g[c->cur],
                                                             c->N, dim, kdx_of(c), c->d_sums);
@@ -188,6 +191,24 @@ template <typename R> static int launch_typed(pond_ctx* c, const void* const* in
   cudaError_t e = cudaMemsetAsync(c->d_sums, 0, sizeof(StepSums), c->stream);
   if (e != cudaSuccess) return cuda_fail(e, "memset sums");
   cudaStream_t s = c->stream;
+  if (c->p.ddf) {  // energy populations: D1Q5 only (pond_create checks), context buffers only
+    if (in) return set_error(POND_ERR_UNSUPPORTED, "explicit step buffers carry no energy populations");
+    a.h_in = (const R*)c->h[i];
+    a.h_out = (R*)c->h[o];
+    a.dof = c->p.ddf_dof;
+    const unsigned g1 = (unsigned)((a.nx + 127) / 128);
+    switch (c->p.interp) {
+      case POND_LAGR2: pull_1d_energy_kernel<POND_LAGR2, R><<<g1, 128, 0, s>>>(a); break;
+      case POND_LAGR3: pull_1d_energy_kernel<POND_LAGR3, R><<<g1, 128, 0, s>>>(a); break;
+      case POND_LAGR4: pull_1d_energy_kernel<POND_LAGR4, R><<<g1, 128, 0, s>>>(a); break;
+      case POND_LAGR5: pull_1d_energy_kernel<POND_LAGR5, R><<<g1, 128, 0, s>>>(a); break;
+      case POND_TVD: pull_1d_energy_kernel<POND_TVD, R><<<g1, 128, 0, s>>>(a); break;
+      case POND_WENO5: pull_1d_energy_kernel<POND_WENO5, R><<<g1, 128, 0, s>>>(a); break;
+      default: return set_error(POND_ERR_UNSUPPORTED, "scheme");
+    }
+    e = cudaGetLastError();
+    return e == cudaSuccess ? POND_OK : cuda_fail(e, "step kernel launch");
+  }
   switch (c->p.lattice) {
     case POND_D1Q5:
       switch (c->p.interp) {
