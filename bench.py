@@ -476,11 +476,14 @@ def shock_vortex_state(n, mach=1.5, T1=0.1, eps=0.3, radius=0.05, gamma=5.0 / 3.
 
 def run_configs(steps=5, warmup=2, d3q125_size=48):
     """Step throughput of the other workloads: the D1Q5 Sod tube (float64,
-    TVD, checked against the float64 oracle over the full 500 steps), the
-    D3Q27 Taylor-Green vortex at 128^3 (quadratic, float32) and the D3Q125
+    TVD, 500 steps; at gamma 3 with one population and at gamma 1.4 with the
+    energy populations, each with its L1 distance to the exact Riemann
+    solution; the float64 oracle's own 500-step comparison is a GPU test),
+    the D3Q27 Taylor-Green vortex at 128^3 (quadratic, float32) and the D3Q125
     shock-vortex box (fixed-origin quadratic, float32).  Progress goes to
     stderr."""
     import lbmpond_b200 as pond
+    from tests.riemann import sample
     out = {}
     t_start = time.perf_counter()
 
@@ -489,28 +492,29 @@ def run_configs(steps=5, warmup=2, d3q125_size=48):
 
     # config 1: 1000 nodes on [0,1], dt/dx = 0.1 -> T = 0.01 p/rho (at dt/dx >= 0.2 the
     # TVD iteration of the float64 oracle itself goes non-finite within 20 steps)
-    n, lam2 = 1000, 0.01
+    # the energy populations with 4 extra degrees of freedom give gamma = 1.4
+    n, lam2, nsteps = 1000, 0.01, 500
     left, right = (1.0, 0.0, lam2 * 1.0), (0.125, 0.0, lam2 * 0.1 / 0.125)
-    with pond.Solver(lattice="D1Q5", shape=(n, 1, 1), precision="fp64", interp=pond.TVD, tau=0.55,
-                     bc=("clamp",) * 3) as s:
-        s.init("sod", 0.5, *left, *right)
-        f0, r0, g0 = s.get_state()
-        t0 = time.perf_counter()
-        s.step(500)
-        wall = time.perf_counter() - t0
-        f1, r1, g1 = s.get_state()
-        d = s.diagnostics()
-    note("sod: GPU done")
-    from oracle import oracle as O  # the float64 oracle is the checker of this row
-    st = O.State(f0, r0, g0)
-    for _ in range(500):
-        st, _, _ = O.step(st, 0, (n, 1, 1), interp=7, tau=0.55, bc=(1, 1, 1))
-    note("sod: oracle done")
-    out["sod_d1q5_fp64"] = {"workload": "D1Q5 Sod, 1000 nodes, TVD, tau 0.55, zero-gradient ends, 500 steps, float64",
-                            "ms_per_step_wall": wall / 500 * 1e3,
-                            "max_rel_diff_vs_oracle": {"rho": float(np.abs(r1 - st.rho).max() / np.abs(st.rho).max()),
-                                                       "T": float(np.abs(g1[3] - st.g[3]).max() / np.abs(st.g[3]).max())},
-                            "niter_max_last_step": d["niter_max"]}
+    x = (np.arange(n) - (n / 2 - 0.5)) / nsteps
+    for key, gamma, dof in (("sod_d1q5_fp64", 3.0, None), ("sod_d1q5_fp64_gamma14", 1.4, 4)):
+        with pond.Solver(lattice="D1Q5", shape=(n, 1, 1), precision="fp64", interp=pond.TVD, tau=0.55,
+                         bc=("clamp",) * 3, ddf_dof=dof) as s:
+            s.init("sod", 0.5, *left, *right)
+            t0 = time.perf_counter()
+            s.step(nsteps)
+            wall = time.perf_counter() - t0
+            _, r1, g1 = s.get_state()
+            d = s.diagnostics()
+        er, eu, ep = sample((left[0], left[1], left[0] * left[2]), (right[0], right[1], right[0] * right[2]), gamma, x)
+        out[key] = {"workload": f"D1Q5 Sod, {n} nodes, TVD, tau 0.55, zero-gradient ends, {nsteps} steps, float64, "
+                                f"gamma {gamma:g}" + (f" (energy populations, {dof} extra degrees of freedom)" if dof
+                                                      else " (one population)"),
+                    "ms_per_step_wall": wall / nsteps * 1e3,
+                    "l1_vs_exact_riemann": {"rho": float(np.abs(r1 - er).mean() / er.mean()),
+                                            "u": float(np.abs(g1[0] - eu).mean() / np.abs(eu).mean()),
+                                            "p": float(np.abs(r1 * g1[3] - ep).mean() / ep.mean())},
+                    "niter_max_last_step": d["niter_max"]}
+        note(f"sod gamma {gamma:g} done")
     # config 2: TGV 128^3, Mach 0.5 with gamma 5/3, T0 = TLat/4 (c = 0.5 node/step)
     T0 = (1.0 / 3.0) / 4
     U0 = 0.5 * np.sqrt(5.0 / 3.0 * T0)

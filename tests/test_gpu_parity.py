@@ -101,6 +101,25 @@ def test_sod_shock_d1q5(orc, pond, precision):
     _compare(out, ref, TOL[precision], "sod")
 
 
+def test_sod_tube_500_steps_fp64(orc, pond):
+    """Config 1 in full: the 1000-node D1Q5 Sod tube (TVD, tau 0.55,
+    zero-gradient ends, T = 0.01 p/rho) for 500 float64 steps, against the
+    oracle's 500 steps from the same initial state."""
+    n = 1000
+    left, right = (1.0, 0.0, 0.01), (0.125, 0.0, 0.01 * 0.1 / 0.125)
+    with pond.Solver(lattice="D1Q5", shape=(n, 1, 1), precision="fp64", interp=7, tau=0.55,
+                     bc=("clamp",) * 3) as s:
+        s.init("sod", 0.5, *left, *right)
+        f0, r0, g0 = s.get_state()
+        s.step(500)
+        _, r1, g1 = s.get_state()
+    st = orc.State(f0, r0, g0)
+    for _ in range(500):
+        st, _, _ = orc.step(st, 0, (n, 1, 1), interp=7, tau=0.55, bc=(1, 1, 1))
+    assert np.abs(r1 - st.rho).max() <= 1e-11 * np.abs(st.rho).max()
+    assert np.abs(g1[3] - st.g[3]).max() <= 1e-10 * np.abs(st.g[3]).max()
+
+
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 @pytest.mark.parametrize("bc", [(1, 0, 0), (2, 0, 0), (1, 1, 1), (2, 2, 2), (0, 2, 1)])
 @pytest.mark.parametrize("lat,shape,interp", [(0, (64, 1, 1), 4), (1, (6, 5, 4), 4), (1, (33, 9, 5), 3),
