@@ -284,7 +284,7 @@ __global__ void __launch_bounds__(128) forward_rows_kernel(const float* P, const
 // A node whose 7-node stencil is exactly uniform, or whose predicted change
 // is below `gate`, keeps its previous gauge.
 template <int H, typename R>
-__global__ void __launch_bounds__(128) predict_kernel(const float* P, const float* stats, const R* rho, const R* g,
+__global__ void __launch_bounds__(128, H == 64 ? 4 : 2) predict_kernel(const float* P, const float* stats, const R* rho, const R* g,
                                                       const R* g_old, long long N, int nx, int ny, int nz, int bc0,
                                                       int bc1,
                                                       int bc2, int lattice, float gate, float* guess) {
