@@ -308,7 +308,7 @@ __global__ void __launch_bounds__(THREADS, 1) pull_d3q27_tile_kernel(StepArgs<fl
   NodeSums ns = {0, 0, 0, 0, 0, 0, 0ull, 0ull, 0ull, 0};
   const long long idx = active ? x + (long long)a.nx * (y + (long long)a.ny * z) : 0;
   // the node's current populations live in shared memory between iterations
-  // (the gauge planes are free once the moments are formed: 4 SN floats =
+  // (the gauge planes are free once the staged nodes are transferred: 4 SN floats =
   // 27 THREADS floats), which keeps them out of the loop's registers
   static_assert(4 * SN == 27 * THREADS, "population store must fit the gauge planes");
   float* f0s = sm + 27 * SN + tid;
@@ -429,7 +429,7 @@ __global__ void __launch_bounds__(THREADS, 1) pull_d3q27_tile_kernel(StepArgs<fl
       }
     } else if (!done) {
       // departure points beyond the staged halo: this lane reads global memory
-      // and forms each stencil node's moments itself
+      // and transfers each stencil node into the reference gauge itself
       const unsigned long long ex = hi[0] - lo[0] + 1, ey = hi[1] - lo[1] + 1, ez = hi[2] - lo[2] + 1;
       work += ex * ey * ez * 171 + ex * ey * 171 + ex * 171;
       const bool all3[3] = {true, true, true};
