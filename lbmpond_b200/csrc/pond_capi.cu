@@ -138,11 +138,20 @@ __global__ void fill_kernel(FillArgs a, R* f0, R* rho0, R* g0, R* f1, R* rho1, R
   rho0[n] = R(rho); rho1[n] = R(rho);
   const R gv[4] = {R(ux), R(uy), R(uz), R(T)};
   for (int k = 0; k < 4; k++) { g0[k * a.N + n] = gv[k]; g1[k * a.N + n] = gv[k]; }
-  if (h0) {  // equilibrium energy populations (D1Q5)
+  if (h0) {  // equilibrium energy populations, class order -> reference order
     const double U[3] = {ux, uy, uz};
-    R h[5];
-    energy_equilibrium<R>(rho, U, T, a.dof, h);
-    for (int q = 0; q < 5; q++) { h0[(long long)q * a.N + n] = h[q]; h1[(long long)q * a.N + n] = h[q]; }
+    R h[27];
+    if (a.Q == 5) {
+      energy_equilibrium<POND_D1Q5, R>(rho, U, T, a.dof, h);
+      for (int q = 0; q < 5; q++) { h0[(long long)q * a.N + n] = h[q]; h1[(long long)q * a.N + n] = h[q]; }
+    } else {
+      energy_equilibrium<POND_D3Q27, R>(rho, U, T, a.dof, h);
+      for (int t = 0; t < 27; t++) {
+        const long long q = Lattice<POND_D3Q27>::ref(t / 9, (t / 3) % 3, t % 3);
+        h0[q * a.N + n] = h[t];
+        h1[q * a.N + n] = h[t];
+      }
+    }
   }
 }
 
@@ -213,8 +222,10 @@ int pond_create(const pond_params* p, pond_ctx** out) {
     return set_error(POND_ERR_UNSUPPORTED, "TVD/WENO5 run on 1D grids (Ny = Nz = 1)");
   if (p->ddf != 0 && p->ddf != 1) return set_error(POND_ERR_ARG, "ddf must be 0 or 1");
   if (p->ddf) {
-    if (p->lattice != POND_D1Q5 || p->Ny != 1 || p->Nz != 1)
-      return set_error(POND_ERR_UNSUPPORTED, "energy populations run on D1Q5 1D grids");
+    const bool d1 = p->lattice == POND_D1Q5 && p->Ny == 1 && p->Nz == 1;
+    const bool d27 = p->lattice == POND_D3Q27 && p->interp >= POND_LAGR2 && p->interp <= POND_LAGR5;
+    if (!d1 && !d27)
+      return set_error(POND_ERR_UNSUPPORTED, "energy populations run on D1Q5 1D grids and D3Q27 (Lagrange 2-5)");
     if (p->ddf_dof < 0 || p->ddf_dof > 1000) return set_error(POND_ERR_ARG, "ddf_dof must be in 0..1000");
     if (p->learned) return set_error(POND_ERR_UNSUPPORTED, "the learned start does not carry energy populations");
   }
@@ -335,9 +346,14 @@ int pond_set_state(pond_ctx* c, const double* f, const double* rho, const double
     std::vector<double> hb((size_t)Q * N);
     for (long long n = 0; n < N; n++) {
       const double U[3] = {g[n], g[N + n], g[2 * N + n]};
-      double h[5];
-      energy_equilibrium<double>(rho[n], U, g[3 * N + n], c->p.ddf_dof, h);
-      for (int q = 0; q < Q; q++) hb[(size_t)q * N + n] = h[q];
+      double h[27];
+      if (c->p.lattice == POND_D1Q5) {
+        energy_equilibrium<POND_D1Q5, double>(rho[n], U, g[3 * N + n], c->p.ddf_dof, h);
+        for (int q = 0; q < Q; q++) hb[(size_t)q * N + n] = h[q];
+      } else {
+        energy_equilibrium<POND_D3Q27, double>(rho[n], U, g[3 * N + n], c->p.ddf_dof, h);
+        for (int t = 0; t < 27; t++) hb[(size_t)Lattice<POND_D3Q27>::ref(t / 9, (t / 3) % 3, t % 3) * N + n] = h[t];
+      }
     }
     st = upload(c, hb.data(), (size_t)Q * N, c->h[c->cur]);
   }

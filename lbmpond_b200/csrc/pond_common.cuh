@@ -140,22 +140,25 @@ struct StepSums {
   int pad;
 };
 
-// Arguments of the step kernels.
-// Equilibrium energy populations of one D1Q5 node in the gauge (U, T) for
-// the double-distribution extension: h_i = rho w_i (|v_i|^2 + dof T),
-// v_i = U + sqrt(T/TLat) xi_i (population order = class order for D1Q5).
-template <typename R>
-__host__ __device__ inline void energy_equilibrium(double rho, const double U[3], double T, double dof, R h[5]) {
-  using L = Lattice<POND_D1Q5>;
+// Equilibrium energy populations of one node in the gauge (U, T) for the
+// double-distribution extension, in tensor-class order t = (cx Q1 + cy) Q1 + cz
+// (for D1Q5 the class order is the population order):
+// h_t = rho w_t (|v_t|^2 + dof T), v_t = U + sqrt(T/TLat) xi_t.
+template <int LAT, typename R>
+__host__ __device__ inline void energy_equilibrium(double rho, const double U[3], double T, double dof, R* h) {
+  using L = Lattice<LAT>;
   const double C = sqrt(fabs(T) * (1.0 / L::TLat));
-  const double side = U[1] * U[1] + U[2] * U[2];
 #pragma unroll
-  for (int k = 0; k < 5; k++) {
-    const double vx = C * L::xi1(k) + U[0];
-    h[k] = R(rho * lattice_weight_t<POND_D1Q5>(k) * (vx * vx + side + dof * T));
+  for (int t = 0; t < L::Q; t++) {
+    const int cx = L::D == 1 ? t : t / (L::Q1 * L::Q1);
+    const double vx = C * L::xi1(cx) + U[0];
+    const double vy = (L::D == 1 ? 0.0 : C * L::xi1((t / L::Q1) % L::Q1)) + U[1];
+    const double vz = (L::D == 1 ? 0.0 : C * L::xi1(t % L::Q1)) + U[2];
+    h[t] = R(rho * lattice_weight_t<LAT>(t) * (vx * vx + vy * vy + vz * vz + dof * T));
   }
 }
 
+// Arguments of the step kernels.
 template <typename R> struct StepArgs {
   const R* f_in;   // [Q][N]
   const R* rho_in; // [N]

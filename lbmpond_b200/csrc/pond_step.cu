@@ -8,6 +8,7 @@
 #include "pond_internal.h"
 #include "pond_step_1d.cuh"
 #include "pond_step_1d_energy.cuh"
+#include "pond_step_d3q27_energy.cuh"
 #include "pond_step_d3q125.cuh"
 #include "pond_step_d3q125_tile.cuh"
 #include "pond_step_d3q27.cuh"
@@ -191,11 +192,23 @@ template <typename R> static int launch_typed(pond_ctx* c, const void* const* in
   cudaError_t e = cudaMemsetAsync(c->d_sums, 0, sizeof(StepSums), c->stream);
   if (e != cudaSuccess) return cuda_fail(e, "memset sums");
   cudaStream_t s = c->stream;
-  if (c->p.ddf) {  // energy populations: D1Q5 only (pond_create checks), context buffers only
+  if (c->p.ddf) {  // energy populations: D1Q5 and D3Q27 (pond_create checks), context buffers only
     if (in) return set_error(POND_ERR_UNSUPPORTED, "explicit step buffers carry no energy populations");
     a.h_in = (const R*)c->h[i];
     a.h_out = (R*)c->h[o];
     a.dof = c->p.ddf_dof;
+    if (c->p.lattice == POND_D3Q27) {
+      const dim3 blk(32, 4, 1), grd((a.nx + 31) / 32, (a.ny + 3) / 4, a.nz);
+      switch (c->p.interp) {
+        case POND_LAGR2: pull_d3q27_energy_kernel<2, R><<<grd, blk, 0, s>>>(a); break;
+        case POND_LAGR3: pull_d3q27_energy_kernel<3, R><<<grd, blk, 0, s>>>(a); break;
+        case POND_LAGR4: pull_d3q27_energy_kernel<4, R><<<grd, blk, 0, s>>>(a); break;
+        case POND_LAGR5: pull_d3q27_energy_kernel<5, R><<<grd, blk, 0, s>>>(a); break;
+        default: return set_error(POND_ERR_UNSUPPORTED, "scheme");
+      }
+      e = cudaGetLastError();
+      return e == cudaSuccess ? POND_OK : cuda_fail(e, "step kernel launch");
+    }
     const unsigned g1 = (unsigned)((a.nx + 127) / 128);
     switch (c->p.interp) {
       case POND_LAGR2: pull_1d_energy_kernel<POND_LAGR2, R><<<g1, 128, 0, s>>>(a); break;

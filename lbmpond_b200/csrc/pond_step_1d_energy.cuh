@@ -39,7 +39,7 @@ __global__ void __launch_bounds__(128) pull_1d_energy_kernel(StepArgs<R> a) {
     load_center<POND_D1Q5, R>(a, idx, f0, rho0, U, T);
     const bool base = a.rho_in[idx] == R(0) && a.g_in[idx] == R(0) && a.g_in[a.N + idx] == R(0) &&
                       a.g_in[2 * a.N + idx] == R(0) && a.g_in[3 * a.N + idx] == R(0);
-    if (base) energy_equilibrium<R>(rho0, U, T, a.dof, h0);  // set_base(1, TLat) with its energy
+    if (base) energy_equilibrium<POND_D1Q5, R>(rho0, U, T, a.dof, h0);  // set_base(1, TLat) with its energy
     else
 #pragma unroll
       for (int k = 0; k < Q; k++) h0[k] = a.h_in[(long long)L::ref(k, 0, 0) * a.N + idx];
@@ -210,7 +210,7 @@ __global__ void __launch_bounds__(128) pull_1d_energy_kernel(StepArgs<R> a) {
     }
     // h relaxes toward its equilibrium in the final gauge (the BGK of f in finish_node)
     R heq[Q];
-    energy_equilibrium<R>(double(R(rho0)), U, T, a.dof, heq);
+    energy_equilibrium<POND_D1Q5, R>(double(R(rho0)), U, T, a.dof, heq);
     const R dtau = R(a.dtau);
 #pragma unroll
     for (int k = 0; k < Q; k++) a.h_out[(long long)L::ref(k, 0, 0) * a.N + idx] = h0[k] + dtau * (heq[k] - h0[k]);
