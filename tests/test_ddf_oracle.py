@@ -101,3 +101,29 @@ def test_ddf_needs_dof(orc):
     st = orc.with_energy(orc.State(t.w[:, None] * rho[None, :], rho, g), 0, 1.0)
     with pytest.raises(ValueError):
         orc.step(st, 0, (16, 1, 1), interp=4)
+
+
+@pytest.mark.parametrize("dof,gamma", [(None, 5.0 / 3.0), (2.0, 1.4)])
+def test_d3q27_sound_speed(orc, dof, gamma):
+    """A small isentropic acoustic wave along x on a periodic D3Q27 grid: the
+    velocity mode's zero crossings give the sound speed sqrt(gamma T0), with
+    gamma = 5/3 for one population and 1.4 with dof = 2 energy populations."""
+    L, T0, eps, steps = 32, 0.05, 1e-3, 125
+    x = np.arange(L)
+    rho = 1 + eps * np.sin(2 * np.pi * x / L)
+    T = T0 * (1 + gamma * eps * np.sin(2 * np.pi * x / L)) / rho
+    z = np.zeros(L)
+    t = orc.tables(1)
+    st = orc.State(t.w[:, None] * rho[None, :], rho, np.stack([z, z, z, T]))
+    if dof is not None:
+        st = orc.with_energy(st, 1, dof)
+    u = []
+    for _ in range(steps):
+        st, _, nc = orc.step(st, 1, (L, 1, 1), interp=4, tau=0.6, dof=dof)
+        assert nc == 0
+        u.append(2 / L * np.sum(st.g[0] * np.cos(2 * np.pi * x / L)))
+    u = np.array(u)
+    cross = [k + u[k] / (u[k] - u[k + 1]) for k in range(steps - 1) if u[k] * u[k + 1] < 0]
+    assert len(cross) >= 2
+    c = L / (2 * np.mean(np.diff(cross)))
+    assert abs(c / np.sqrt(gamma * T0) - 1) < 2e-3, (c, np.sqrt(gamma * T0))
