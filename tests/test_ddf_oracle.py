@@ -5,8 +5,8 @@ ratio is gamma = (Dim + dof + 2) / (Dim + dof) instead of the single
 population's (Dim + 2) / Dim.  The reference has only non-compiling
 scaffolding for it (structs.cuh:37-39,336-341,391-394, lbpack.cu:18-20,
 steps.cu:233-236), so these tests pin the extension to physics: equilibrium
-moments, a uniform fixed point, conservation, and the exact Sod solution at
-gamma = 1.4 and gamma = 3.
+moments, a uniform fixed point, conservation, the exact Sod solution at
+gamma = 1.4 and gamma = 3 (D1Q5), and the D3Q27 sound speed at gamma = 5/3 and 1.4.
 """
 import numpy as np
 import pytest
