@@ -140,10 +140,13 @@ __global__ void fill_kernel(FillArgs a, R* f0, R* rho0, R* g0, R* f1, R* rho1, R
   for (int k = 0; k < 4; k++) { g0[k * a.N + n] = gv[k]; g1[k * a.N + n] = gv[k]; }
   if (h0) {  // equilibrium energy populations, class order -> reference order
     const double U[3] = {ux, uy, uz};
-    R h[27];
+    R h[125];
     if (a.Q == 5) {
       energy_equilibrium<POND_D1Q5, R>(rho, U, T, a.dof, h);
       for (int q = 0; q < 5; q++) { h0[(long long)q * a.N + n] = h[q]; h1[(long long)q * a.N + n] = h[q]; }
+    } else if (a.Q == 125) {  // class order is the population order
+      energy_equilibrium<POND_D3Q125, R>(rho, U, T, a.dof, h);
+      for (int q = 0; q < 125; q++) { h0[(long long)q * a.N + n] = h[q]; h1[(long long)q * a.N + n] = h[q]; }
     } else {
       energy_equilibrium<POND_D3Q27, R>(rho, U, T, a.dof, h);
       for (int t = 0; t < 27; t++) {
@@ -224,8 +227,10 @@ int pond_create(const pond_params* p, pond_ctx** out) {
   if (p->ddf) {
     const bool d1 = p->lattice == POND_D1Q5 && p->Ny == 1 && p->Nz == 1;
     const bool d27 = p->lattice == POND_D3Q27 && p->interp >= POND_LAGR2 && p->interp <= POND_LAGR5;
-    if (!d1 && !d27)
-      return set_error(POND_ERR_UNSUPPORTED, "energy populations run on D1Q5 1D grids and D3Q27 (Lagrange 2-5)");
+    const bool d125 = p->lattice == POND_D3Q125 && p->precision == POND_FP32;
+    if (!d1 && !d27 && !d125)
+      return set_error(POND_ERR_UNSUPPORTED,
+                       "energy populations run on D1Q5 1D grids, D3Q27 (Lagrange 2-5) and D3Q125 (float32)");
     if (p->ddf_dof < 0 || p->ddf_dof > 1000) return set_error(POND_ERR_ARG, "ddf_dof must be in 0..1000");
     if (p->learned) return set_error(POND_ERR_UNSUPPORTED, "the learned start does not carry energy populations");
   }
@@ -346,9 +351,12 @@ int pond_set_state(pond_ctx* c, const double* f, const double* rho, const double
     std::vector<double> hb((size_t)Q * N);
     for (long long n = 0; n < N; n++) {
       const double U[3] = {g[n], g[N + n], g[2 * N + n]};
-      double h[27];
+      double h[125];
       if (c->p.lattice == POND_D1Q5) {
         energy_equilibrium<POND_D1Q5, double>(rho[n], U, g[3 * N + n], c->p.ddf_dof, h);
+        for (int q = 0; q < Q; q++) hb[(size_t)q * N + n] = h[q];
+      } else if (c->p.lattice == POND_D3Q125) {
+        energy_equilibrium<POND_D3Q125, double>(rho[n], U, g[3 * N + n], c->p.ddf_dof, h);
         for (int q = 0; q < Q; q++) hb[(size_t)q * N + n] = h[q];
       } else {
         energy_equilibrium<POND_D3Q27, double>(rho[n], U, g[3 * N + n], c->p.ddf_dof, h);

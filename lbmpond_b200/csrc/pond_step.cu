@@ -197,6 +197,20 @@ template <typename R> static int launch_typed(pond_ctx* c, const void* const* in
     a.h_in = (const R*)c->h[i];
     a.h_out = (R*)c->h[o];
     a.dof = c->p.ddf_dof;
+    if (c->p.lattice == POND_D3Q125) {
+      if constexpr (std::is_same<R, float>::value) {
+        const size_t smem = sizeof(d125t::SmemT<true>);
+        e = cudaFuncSetAttribute(d125t::pull_d3q125_tile_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+        const dim3 grd((a.nx + d125t::T - 1) / d125t::T, (a.ny + d125t::T - 1) / d125t::T,
+                       (a.nz + d125t::T - 1) / d125t::T);
+        d125t::pull_d3q125_tile_kernel<true><<<grd, d125t::THREADS, smem, s>>>(a);
+        e = cudaGetLastError();
+        return e == cudaSuccess ? POND_OK : cuda_fail(e, "step kernel launch");
+      }
+      return set_error(POND_ERR_UNSUPPORTED, "energy populations on D3Q125 run in float32");
+    }
     if (c->p.lattice == POND_D3Q27) {
       const dim3 blk(32, 4, 1), grd((a.nx + 31) / 32, (a.ny + 3) / 4, a.nz);
       switch (c->p.interp) {
@@ -263,11 +277,12 @@ template <typename R> static int launch_typed(pond_ctx* c, const void* const* in
     case POND_D3Q125: {
       if constexpr (std::is_same<R, float>::value) {
         const size_t smem = sizeof(d125t::Smem);
-        e = cudaFuncSetAttribute(d125t::pull_d3q125_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = cudaFuncSetAttribute(d125t::pull_d3q125_tile_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
         if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
         const dim3 grd((a.nx + d125t::T - 1) / d125t::T, (a.ny + d125t::T - 1) / d125t::T,
                        (a.nz + d125t::T - 1) / d125t::T);
-        d125t::pull_d3q125_tile_kernel<<<grd, d125t::THREADS, smem, s>>>(a);
+        d125t::pull_d3q125_tile_kernel<false><<<grd, d125t::THREADS, smem, s>>>(a);
       } else {  // float64: one CTA per node, as the reference kernel
         const size_t smem = sizeof(D125Smem<R>);
         e = cudaFuncSetAttribute(pull_d3q125_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -44,15 +44,18 @@ constexpr int PS = SN + 1;          // plane stride: 25 * 217 = 17 mod 32
 constexpr int WARPS = 8;
 constexpr int THREADS = 32 * WARPS;
 
-struct Smem {
+template <bool kE> struct SmemT {
   float f[125 * PS];       // staged populations (non-finite values zeroed), then their transfer into R
+  float h[kE ? 125 * PS : 1];  // the same for the energy populations (double-distribution extension)
   float u[3][SN];          // staged velocities (sign-flipped on mirrored axes)
   float c[SN];             // sqrts(T / TLat)
   unsigned char flags[SN]; // mirrored axes (bits 0-2)
   float GY[WARPS][3][25];  // per warp and iteration: y weight x transfer entry, [n_y][5 i2 + k2]
 };
+using Smem = SmemT<false>;
 
-static_assert(2 * (sizeof(Smem) + 1024) <= 233472, "two CTAs must fit in the 228 KB of an SM");
+static_assert(2 * (sizeof(SmemT<false>) + 1024) <= 233472, "two CTAs must fit in the 228 KB of an SM");
+static_assert(sizeof(SmemT<true>) + 1024 <= 233472, "the energy variant must fit one CTA per SM");
 
 // global node of staged node i and its mirror flags
 __device__ __forceinline__ int staged_global(const StepArgs<float>& a, int x0, int y0, int z0, int i, bool rv[3]) {
@@ -93,10 +96,13 @@ __device__ __forceinline__ void stencil_weights(int pos, double C, double U, int
   lagr_weights<3, float>(crd - double(pos - 1), w);
 }
 
-__global__ void __launch_bounds__(THREADS, 2) pull_d3q125_tile_kernel(StepArgs<float> a) {
+// kE: with the energy populations of the double-distribution extension
+// (staged, transferred and contracted like f; T from their sum; one CTA per SM)
+template <bool kE>
+__global__ void __launch_bounds__(THREADS, kE ? 1 : 2) pull_d3q125_tile_kernel(StepArgs<float> a) {
   using L = Lattice<POND_D3Q125>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
+  SmemT<kE>& sm = *reinterpret_cast<SmemT<kE>*>(smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int x0 = blockIdx.x * T, y0 = blockIdx.y * T, z0 = blockIdx.z * T;
 
@@ -120,6 +126,11 @@ __global__ void __launch_bounds__(THREADS, 2) pull_d3q125_tile_kernel(StepArgs<f
     const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(&sm.f[p * PS + i]));
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(a.f_in + (long long)p * a.N + g)
                  : "memory");
+    if constexpr (kE) {
+      const unsigned dh = static_cast<unsigned>(__cvta_generic_to_shared(&sm.h[p * PS + i]));
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dh), "l"(a.h_in + (long long)p * a.N + g)
+                   : "memory");
+    }
   }
   asm volatile("cp.async.wait_all;\n" ::: "memory");
   __syncthreads();
@@ -127,6 +138,7 @@ __global__ void __launch_bounds__(THREADS, 2) pull_d3q125_tile_kernel(StepArgs<f
     const int p = idx / SN, i = idx - p * SN;
     float& v = sm.f[p * PS + i];
     v = finite_or_zero_f(v);
+    if constexpr (kE) sm.h[p * PS + i] = finite_or_zero_f(sm.h[p * PS + i]);
   }
   __syncthreads();
 
@@ -164,8 +176,11 @@ __global__ void __launch_bounds__(THREADS, 2) pull_d3q125_tile_kernel(StepArgs<f
         rq[ax] = ((fl >> ax) & 1 ? -cn : cn) * icref;
       }
       float* fi = sm.f + i;
+      float* hi = kE ? sm.h + i : nullptr;
       if (!ok) {
         for (int pp = 0; pp < 125; pp++) fi[pp * PS] = 0.f;
+        if constexpr (kE)
+          for (int pp = 0; pp < 125; pp++) hi[pp * PS] = 0.f;
         continue;
       }
 #pragma unroll
@@ -193,6 +208,19 @@ __global__ void __launch_bounds__(THREADS, 2) pull_d3q125_tile_kernel(StepArgs<f
           }
 #pragma unroll
           for (int ii = 0; ii < 5; ii++) fi[(base + ii * st) * PS] = w[ii];
+          if constexpr (kE) {
+#pragma unroll
+            for (int b = 0; b < 5; b++) v[b] = hi[(base + b * st) * PS];
+#pragma unroll
+            for (int ii = 0; ii < 5; ii++) {
+              float t = B[ii][0] * v[0];
+#pragma unroll
+              for (int b = 1; b < 5; b++) t = fmaf(B[ii][b], v[b], t);
+              w[ii] = t;
+            }
+#pragma unroll
+            for (int ii = 0; ii < 5; ii++) hi[(base + ii * st) * PS] = w[ii];
+          }
         }
       }
     }
@@ -211,9 +239,12 @@ __global__ void __launch_bounds__(THREADS, 2) pull_d3q125_tile_kernel(StepArgs<f
     if (x >= a.nx || y >= a.ny || z >= a.nz) continue;  // warp-uniform
     const long long idx = x + (long long)a.nx * (y + (long long)a.ny * z);
     // c0.load of the centre: this lane's populations (j, iy, k), iy = 0..4
-    float f0[5];
+    float f0[5], h0[5];
 #pragma unroll
-    for (int iy = 0; iy < 5; iy++) f0[iy] = worker ? a.f_in[(long long)(25 * j + 5 * iy + k) * a.N + idx] : 0.f;
+    for (int iy = 0; iy < 5; iy++) {
+      f0[iy] = worker ? a.f_in[(long long)(25 * j + 5 * iy + k) * a.N + idx] : 0.f;
+      h0[iy] = (kE && worker) ? a.h_in[(long long)(25 * j + 5 * iy + k) * a.N + idx] : 0.f;
+    }
     double rho0 = a.rho_in[idx];
     double U[3] = {(double)a.g_in[idx], (double)a.g_in[a.N + idx], (double)a.g_in[2 * a.N + idx]};
     double Tc = a.g_in[3 * a.N + idx];
@@ -221,7 +252,14 @@ __global__ void __launch_bounds__(THREADS, 2) pull_d3q125_tile_kernel(StepArgs<f
       rho0 = 1;
       Tc = L::TLat;
 #pragma unroll
-      for (int iy = 0; iy < 5; iy++) f0[iy] = worker ? float(lattice_weight_t<POND_D3Q125>(25 * j + 5 * iy + k)) : 0.f;
+      for (int iy = 0; iy < 5; iy++) {
+        const double w = lattice_weight_t<POND_D3Q125>(25 * j + 5 * iy + k);
+        f0[iy] = worker ? float(w) : 0.f;
+        if constexpr (kE) {  // its energy at equilibrium: w (|xi|^2 + dof TLat)
+          const double v2 = xi5(j) * xi5(j) + xi5(iy) * xi5(iy) + xi5(k) * xi5(k);
+          h0[iy] = worker ? float(w * (v2 + a.dof * L::TLat)) : 0.f;
+        }
+      }
     }
     if (a.guess) {
       U[0] = a.guess[idx]; U[1] = a.guess[a.N + idx]; U[2] = a.guess[2 * a.N + idx]; Tc = a.guess[3 * a.N + idx];
@@ -230,7 +268,7 @@ __global__ void __launch_bounds__(THREADS, 2) pull_d3q125_tile_kernel(StepArgs<f
     const int qc = ((lz + 1) * S + (ly + 1)) * S + (lx + 1);  // staged centre
     int niter = 0;
     bool conv = false;
-    float acc[5];
+    float acc[5], acch[5];
     while (niter < a.max_iter) {
       niter++;
       const double C = sqrt(Tc / L::TLat);
@@ -263,13 +301,15 @@ __global__ void __launch_bounds__(THREADS, 2) pull_d3q125_tile_kernel(StepArgs<f
       }
       __syncwarp();
 #pragma unroll
-      for (int iy = 0; iy < 5; iy++) acc[iy] = 0.f;
+      for (int iy = 0; iy < 5; iy++) { acc[iy] = 0.f; acch[iy] = 0.f; }
 #pragma unroll
       for (int nx = 0; nx < 3; nx++) {
         float Yr[5] = {0.f, 0.f, 0.f, 0.f, 0.f};  // (j, i2, k) of the row
+        float Yh[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll 1
         for (int ny = 0; ny < 3; ny++) {
           float Zc[5] = {0.f, 0.f, 0.f, 0.f, 0.f};  // (j, k2, k) of the column
+          float Zh[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll 1
           for (int nz = 0; nz < 3; nz++) {
             const float wn = nz == 0 ? wz[0] : nz == 1 ? wz[1] : wz[2];
@@ -281,26 +321,42 @@ __global__ void __launch_bounds__(THREADS, 2) pull_d3q125_tile_kernel(StepArgs<f
             for (int k2 = 0; k2 < 5; k2++)
 #pragma unroll
               for (int k3 = 0; k3 < 5; k3++) Zc[k2] = fmaf(gz[k3], fq[(5 * k2 + k3) * PS], Zc[k2]);
+            if constexpr (kE) {
+              const float* hq = sm.h + (fq - sm.f);
+#pragma unroll
+              for (int k2 = 0; k2 < 5; k2++)
+#pragma unroll
+                for (int k3 = 0; k3 < 5; k3++) Zh[k2] = fmaf(gz[k3], hq[(5 * k2 + k3) * PS], Zh[k2]);
+            }
           }
           const float* gy = sm.GY[warp][ny];
 #pragma unroll
           for (int i2 = 0; i2 < 5; i2++)
 #pragma unroll
-            for (int k2 = 0; k2 < 5; k2++) Yr[i2] = fmaf(gy[5 * i2 + k2], Zc[k2], Yr[i2]);
+            for (int k2 = 0; k2 < 5; k2++) {
+              Yr[i2] = fmaf(gy[5 * i2 + k2], Zc[k2], Yr[i2]);
+              if constexpr (kE) Yh[i2] = fmaf(gy[5 * i2 + k2], Zh[k2], Yh[i2]);
+            }
         }
 #pragma unroll
         for (int k1 = 0; k1 < 5; k1++) {
           const float g = wx[nx] * tx[k1];
 #pragma unroll
-          for (int i2 = 0; i2 < 5; i2++) acc[i2] = fmaf(g, __shfl_sync(0xffffffffu, Yr[i2], 5 * k1 + k), acc[i2]);
+          for (int i2 = 0; i2 < 5; i2++) {
+            acc[i2] = fmaf(g, __shfl_sync(0xffffffffu, Yr[i2], 5 * k1 + k), acc[i2]);
+            if constexpr (kE) acch[i2] = fmaf(g, __shfl_sync(0xffffffffu, Yh[i2], 5 * k1 + k), acch[i2]);
+          }
         }
       }
       if (!(C >= 1.0e-300)) {  // target T = 0: every transfer term is non-finite and dropped
 #pragma unroll
-        for (int iy = 0; iy < 5; iy++) acc[iy] = 0.f;
+        for (int iy = 0; iy < 5; iy++) { acc[iy] = 0.f; acch[iy] = 0.f; }
       }
       // calcMoments in float64 (structs.cuh:315-342), warp-wide
-      double mv[5] = {0, 0, 0, 0, 0};
+      constexpr int NM = kE ? 6 : 5;
+      double mv[NM];
+#pragma unroll
+      for (int q = 0; q < NM; q++) mv[q] = 0;
       if (worker) {
         const double vx = C * xi5(j) + U[0], vz = C * xi5(k) + U[2];
 #pragma unroll
@@ -308,20 +364,22 @@ __global__ void __launch_bounds__(THREADS, 2) pull_d3q125_tile_kernel(StepArgs<f
           const double fv = acc[iy], vy = C * xi5(iy) + U[1];
           mv[0] += fv; mv[1] += fv * vx; mv[2] += fv * vy; mv[3] += fv * vz;
           mv[4] += fv * (vx * vx + vy * vy + vz * vz);
+          if constexpr (kE) mv[NM - 1] += double(acch[iy]);
         }
       }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1)
 #pragma unroll
-        for (int m = 0; m < 5; m++) mv[m] += __shfl_xor_sync(0xffffffffu, mv[m], o);
+        for (int m = 0; m < NM; m++) mv[m] += __shfl_xor_sync(0xffffffffu, mv[m], o);
       const double rho = mv[0];
-      double m[4] = {mv[1], mv[2], mv[3], mv[4]};
+      double m[4] = {mv[1], mv[2], mv[3], kE ? mv[NM - 1] : mv[4]};
       if (rho != 0) {
         const double ir = 1.0 / rho;
 #pragma unroll
         for (int q = 0; q < 4; q++) m[q] *= ir;
       }
-      double Tn = (m[3] - m[0] * m[0] - m[1] * m[1] - m[2] * m[2]) * (1.0 / L::Dim);
+      // T from the second moment of f, or with energy populations from their sum
+      double Tn = (m[3] - m[0] * m[0] - m[1] * m[1] - m[2] * m[2]) / (L::Dim + (kE ? a.dof : 0.0));
       if (Tn < 0) Tn = Tc;  // steps.cu:475
       bool ok = true;
 #pragma unroll
@@ -332,10 +390,14 @@ __global__ void __launch_bounds__(THREADS, 2) pull_d3q125_tile_kernel(StepArgs<f
         for (int iy = 0; iy < 5; iy++) {
           const double nv = acc[iy], ov = f0[iy];
           ok = ok && !(fabs(nv - ov) >= a.tol_abs + a.tol_rel * fabs(nv));
+          if constexpr (kE) {
+            const double nh = acch[iy], oh = h0[iy];
+            ok = ok && !(fabs(nh - oh) >= a.tol_abs + a.tol_rel * fabs(nh));
+          }
         }
       const bool all_ok = __all_sync(0xffffffffu, ok);
 #pragma unroll
-      for (int iy = 0; iy < 5; iy++) f0[iy] = acc[iy];
+      for (int iy = 0; iy < 5; iy++) { f0[iy] = acc[iy]; h0[iy] = acch[iy]; }
       rho0 = rho; U[0] = m[0]; U[1] = m[1]; U[2] = m[2]; Tc = Tn;
       if (all_ok) { conv = true; break; }
     }
@@ -347,6 +409,13 @@ __global__ void __launch_bounds__(THREADS, 2) pull_d3q125_tile_kernel(StepArgs<f
         const int p = 25 * j + 5 * iy + k;
         const float fb = f0[iy] + dtau * (rr * float(lattice_weight_t<POND_D3Q125>(p)) - f0[iy]);
         a.f_out[(long long)p * a.N + idx] = fb;
+        if constexpr (kE) {  // h toward rho w (|v|^2 + dof T) in the final gauge
+          const double Cf = sqrt(fabs(Tc) * (1.0 / L::TLat));
+          const double vx = Cf * xi5(j) + U[0], vy = Cf * xi5(iy) + U[1], vz = Cf * xi5(k) + U[2];
+          const float heq = float(double(rr) * lattice_weight_t<POND_D3Q125>(p) *
+                                  (vx * vx + vy * vy + vz * vz + a.dof * Tc));
+          a.h_out[(long long)p * a.N + idx] = h0[iy] + dtau * (heq - h0[iy]);
+        }
       }
     if (lane == 0) {
       const float u0 = float(U[0]), u1 = float(U[1]), u2 = float(U[2]), ts = float(Tc);
@@ -356,7 +425,7 @@ __global__ void __launch_bounds__(THREADS, 2) pull_d3q125_tile_kernel(StepArgs<f
       const double dr = rr, d0 = u0, d1 = u1, d2 = u2, dt = ts;
       const double u2s = d0 * d0 + d1 * d1 + d2 * d2;
       ns.mass += dr; ns.m0 += dr * d0; ns.m1 += dr * d1; ns.m2 += dr * d2;
-      ns.enrg += dr * (u2s + L::Dim * dt);
+      ns.enrg += dr * (u2s + (L::Dim + (kE ? a.dof : 0.0)) * dt);
       ns.k += a.kdx * u2s;
       ns.niter += niter; ns.nonconv += conv ? 0 : 1; ns.nmax = max(ns.nmax, niter);
       ns.work += 27ull * niter;

@@ -1,7 +1,8 @@
 """GPU parity of the double-distribution extension (energy populations) with
 the float64 oracle, through the C ABI.
 
-A D1Q5 or D3Q27 context made with ``ddf_dof`` carries energy populations h beside f;
+A D1Q5, D3Q27 or (float32) D3Q125 context made with ``ddf_dof`` carries energy
+populations h beside f;
 its temperature comes from them and gamma = (Dim + dof + 2) / (Dim + dof).
 The oracle restates the same extension (``orc.step(..., dof=...)``); both are
 pinned to physics by ``tests/test_ddf_oracle.py`` (exact Riemann solutions).
@@ -95,6 +96,32 @@ def test_d3q27_energy_step_matches_oracle(orc, pond, interp, shape, bc, precisio
     assert abs(d["enrg"] - total) <= 1e-6 * abs(total)
 
 
+@pytest.mark.parametrize("shape,bc", [((5, 4, 4), (0, 0, 0)), ((9, 6, 5), (1, 0, 2))])
+def test_d3q125_energy_step_matches_oracle(orc, pond, shape, bc):
+    """The staged D3Q125 tile kernel with energy populations (float32)."""
+    dof, tau = 2, 0.9
+    rho, g = smooth_state(shape, 3, seed=5, modes=1, du=0.03)
+    f = perturbed_populations(orc, 2, rho, g, seed=5, eps=0.01)
+    st = orc.with_energy(orc.State(f, rho, g), 2, dof)
+    st.h = st.h * (1 + 0.01 * np.random.default_rng(9).standard_normal(st.h.shape))
+    names = {0: "periodic", 1: "clamp", 2: "mirror"}
+    with pond.Solver(lattice="D3Q125", shape=shape, precision="fp32", tau=tau,
+                     bc=tuple(names[b] for b in bc), ddf_dof=dof) as s:
+        s.set_state(st.rho, st.g, f=st.f)
+        s.set_energy(st.h)
+        ref = st
+        for _ in range(2):
+            s.step(1)
+            ref, niter, nc = orc.step(ref, 2, shape, interp=6, tau=tau, bc=bc, dof=dof,
+                                      tol_abs=s.params.tol_abs, tol_rel=s.params.tol_rel)
+        err = _errors(s, ref)
+        d = s.diagnostics()
+    assert all(v <= TOL["fp32"] for v in err.values()), err
+    assert d["nonconverged"] == 0
+    total = np.sum(ref.rho * (np.sum(ref.g[:3] ** 2, axis=0) + (3 + dof) * ref.g[3]))
+    assert abs(d["enrg"] - total) <= 1e-6 * abs(total)
+
+
 def test_sod_gamma_14_on_the_gpu(orc, pond):
     """200 float64 steps of the 400-node Sod tube with dof = 4: the same
     state as the oracle, and the exact gamma = 1.4 solution to 1.5 % (L1)."""
@@ -135,5 +162,5 @@ def test_energy_api(orc, pond):
         s.set_state(rho, g)
         with pytest.raises(pond._lib.PondError):
             s.get_energy()
-    with pytest.raises(pond._lib.PondError):  # the staged D3Q125 kernel has no energy variant
-        pond.Solver(lattice="D3Q125", shape=(4, 4, 4), ddf_dof=2)
+    with pytest.raises(pond._lib.PondError):  # D3Q125 energy populations run in float32 only
+        pond.Solver(lattice="D3Q125", shape=(4, 4, 4), precision="fp64", ddf_dof=2)
