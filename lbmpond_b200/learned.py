@@ -94,16 +94,32 @@ def collect_pairs(solver, X, Y, offset_rows=0, stride=7, seed=0, nodes=None):
     """Append the pairs of the solver's last step to rows [offset_rows, ...)
     of the torch buffers X [cap, 39] and Y [cap, 4] (and their node indices
     to the int64 buffer `nodes`, if given); returns rows written."""
+    import torch
     L = _lib.load()
     cap = X.shape[0] - offset_rows
     if cap <= 0:
         return 0
+    if nodes is None:  # the node of every row, to put the rows in a repeatable order
+        nodes_all = torch.empty(cap, dtype=torch.int64, device=X.device)
+        base = 0
+    else:
+        nodes_all, base = nodes, offset_rows
     n = ctypes.c_int64()
     xp = X.data_ptr() + offset_rows * NIN * 4
     yp = Y.data_ptr() + offset_rows * NOUT * 4
-    np_ = nodes.data_ptr() + offset_rows * 8 if nodes is not None else None
+    np_ = nodes_all.data_ptr() + base * 8
     _lib.check(L.pond_collect_pairs(solver.handle, xp, yp, np_, int(cap), int(stride), int(seed), ctypes.byref(n)))
-    return int(n.value)
+    n = int(n.value)
+    if n > 1:  # the kernel appends rows in arrival order: sort them by node, then shuffle with the seed
+        rows = slice(offset_rows, offset_rows + n)
+        gen = torch.Generator(device=X.device)
+        gen.manual_seed(int(seed))
+        order = torch.argsort(nodes_all[base:base + n])
+        order = order[torch.randperm(n, generator=gen, device=X.device)]
+        X[rows] = X[rows][order]
+        Y[rows] = Y[rows][order]
+        nodes_all[base:base + n] = nodes_all[base:base + n][order]
+    return n
 
 
 def calibrate_gate(net, X, Y, tol=1e-6, candidates=(0.0, 1e-6, 3e-6, 1e-5, 3e-5, 1e-4, 3e-4, 1e-3, 3e-3, 1e-2,
