@@ -602,7 +602,7 @@ def main():
     ap.add_argument("--collect-steps", type=int, default=30, help="spin-up steps that feed training pairs")
     ap.add_argument("--pair-stride", type=int, default=61)
     ap.add_argument("--pair-capacity", type=int, default=4_000_000)
-    ap.add_argument("--train-steps", type=int, default=3000)
+    ap.add_argument("--train-steps", type=int, default=10000)
     ap.add_argument("--no-l1", action="store_true")
     ap.add_argument("--l1-steps", type=int, default=3)
     ap.add_argument("--ref-size", type=int, default=24)
