@@ -525,6 +525,20 @@ def run_configs(steps=5, warmup=2, d3q125_size=48):
                                 "ms_per_step": ms, "MLUPS": 128 ** 3 / ms / 1e3, "niter_mean": d["niter_mean"],
                                 "niter_max": d["niter_max"], "steps_timed": f"{warmup + 1}..{warmup + steps}"}
     note("tgv done")
+    # the same vortex as a gamma = 1.4 gas: energy populations with 2 extra degrees of freedom
+    # (one thread per node: the staged tile kernel has no room for them)
+    T14 = (1.0 / 3.0) / 4
+    U14 = 0.5 * np.sqrt(1.4 * T14)
+    with pond.Solver(lattice="D3Q27", shape=(128,) * 3, precision="fp32", interp=pond.LAGR3, tau=0.51,
+                     ddf_dof=2) as s:
+        s.init("tgv", U14, T14, 1.0, 1.4)
+        ms, d = _time_steps(s, steps, warmup)
+        out["tgv_d3q27_128_gamma14"] = {
+            "workload": "D3Q27 Taylor-Green 128^3, Mach 0.5, quadratic Lagrange, tau 0.51, float32, gamma 1.4 "
+                        "(energy populations, 2 extra degrees of freedom)",
+            "ms_per_step": ms, "MLUPS": 128 ** 3 / ms / 1e3, "niter_mean": d["niter_mean"], "niter_max": d["niter_max"],
+            "steps_timed": f"{warmup + 1}..{warmup + steps}"}
+    note("tgv gamma 1.4 done")
     # config 5: D3Q125 shock + vortex, plain and learned start from the same spun-up state
     import torch
     from lbmpond_b200.learned import Predictor, attach, calibrate_gate, collect_pairs, keep_history
@@ -568,6 +582,19 @@ def run_configs(steps=5, warmup=2, d3q125_size=48):
                         "network": "39-128-128-4", "pairs": rows, "loss_first": float(loss[0]),
                         "loss_last": float(loss[-1]), "gate": gate},
             "l1_rho_learned_vs_plain": float(np.abs(rho_l - rho_p).mean() / np.abs(rho_p).mean())}
+    # the shock + vortex problem for a gamma = 1.4 gas: energy populations with 2 extra degrees of
+    # freedom and the Rankine-Hugoniot states and isentropic vortex of gamma 1.4
+    with pond.Solver(**kw, ddf_dof=2) as s:
+        rho, g = shock_vortex_state(m, gamma=1.4)
+        s.set_state(rho, g)
+        s.step(8)
+        ms_e, d_e = _time_steps(s, max(1, steps // 2), 1)
+    out["shock_vortex_d3q125_energy"] = {
+        "workload": f"D3Q125 {m}^3 Mach 1.5 shock + isentropic vortex at gamma 1.4 (energy populations, 2 extra "
+                    "degrees of freedom), float32, after 8 steps",
+        "ms_per_step": ms_e, "MLUPS": m ** 3 / ms_e / 1e3, "niter_mean": d_e["niter_mean"],
+        "niter_max": d_e["niter_max"], "nonconverged": d_e["nonconverged"]}
+    note("d3q125 energy populations timed")
     return out
 
 
