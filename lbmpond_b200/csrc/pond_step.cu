@@ -9,7 +9,6 @@
 #include "pond_step_1d.cuh"
 #include "pond_step_1d_energy.cuh"
 #include "pond_step_d3q27_energy.cuh"
-#include "pond_step_d3q125.cuh"
 #include "pond_step_d3q125_tile.cuh"
 #include "pond_step_d3q27.cuh"
 #include "pond_step_point.cuh"
@@ -274,21 +273,14 @@ template <typename R> static int launch_typed(pond_ctx* c, const void* const* in
         default: return set_error(POND_ERR_UNSUPPORTED, "scheme");
       }
       break;
-    case POND_D3Q125: {
-      if constexpr (std::is_same<R, float>::value) {
-        const size_t smem = sizeof(d125t::Smem);
-        e = cudaFuncSetAttribute(d125t::pull_d3q125_tile_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
-        const dim3 grd((a.nx + d125t::T - 1) / d125t::T, (a.ny + d125t::T - 1) / d125t::T,
-                       (a.nz + d125t::T - 1) / d125t::T);
-        d125t::pull_d3q125_tile_kernel<false><<<grd, d125t::THREADS, smem, s>>>(a);
-      } else {  // float64: one CTA per node, as the reference kernel
-        const size_t smem = sizeof(D125Smem<R>);
-        e = cudaFuncSetAttribute(pull_d3q125_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
-        pull_d3q125_kernel<R><<<(unsigned)c->N, D125_THREADS, smem, s>>>(a);
-      }
+    case POND_D3Q125: {  // staged tile, reference-gauge transfer (float64: one CTA per SM)
+      const size_t smem = sizeof(d125t::SmemT<false, R>);
+      e = cudaFuncSetAttribute(d125t::pull_d3q125_tile_kernel<false, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem);
+      if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+      const dim3 grd((a.nx + d125t::T - 1) / d125t::T, (a.ny + d125t::T - 1) / d125t::T,
+                     (a.nz + d125t::T - 1) / d125t::T);
+      d125t::pull_d3q125_tile_kernel<false, R><<<grd, d125t::THREADS, smem, s>>>(a);
       break;
     }
     default: return set_error(POND_ERR_UNSUPPORTED, "lattice");

@@ -1,9 +1,9 @@
-// D3Q125 PonD pull step, float32: a tile of nodes per CTA, a warp per node.
+// D3Q125 PonD pull step, float32 or float64: a tile of nodes per CTA, a warp
+// per node.
 //
-// Same arithmetic as pull_d3q125_kernel (steps.cu:151-250 PonDstepD3Q125:
-// quadratic stencil with its origin fixed at coord-1, gauge transfer by the
-// 5-point Lagrange basis, float64 moments and convergence test), organised
-// for the SM:
+// The arithmetic of steps.cu:151-250 PonDstepD3Q125 (quadratic stencil with
+// its origin fixed at coord-1, gauge transfer by the 5-point Lagrange basis,
+// float64 moments and convergence test), organised for the SM:
 //
 //  * a CTA owns a 4 x 4 x 4 tile and stages it with its +-1 halo (6 x 6 x 6
 //    nodes: 125 population planes, the gauge velocities and c, 113 KB) once
@@ -44,21 +44,23 @@ constexpr int PS = SN + 1;          // plane stride: 25 * 217 = 17 mod 32
 constexpr int WARPS = 8;
 constexpr int THREADS = 32 * WARPS;
 
-template <bool kE> struct SmemT {
-  float f[125 * PS];       // staged populations (non-finite values zeroed), then their transfer into R
-  float h[kE ? 125 * PS : 1];  // the same for the energy populations (double-distribution extension)
-  float u[3][SN];          // staged velocities (sign-flipped on mirrored axes)
-  float c[SN];             // sqrts(T / TLat)
+template <bool kE, typename Rs = float> struct SmemT {
+  Rs f[125 * PS];          // staged populations (non-finite values zeroed), then their transfer into R
+  Rs h[kE ? 125 * PS : 1]; // the same for the energy populations (double-distribution extension)
+  Rs u[3][SN];             // staged velocities (sign-flipped on mirrored axes)
+  Rs c[SN];                // sqrts(T / TLat)
   unsigned char flags[SN]; // mirrored axes (bits 0-2)
-  float GY[WARPS][3][25];  // per warp and iteration: y weight x transfer entry, [n_y][5 i2 + k2]
+  Rs GY[WARPS][3][25];     // per warp and iteration: y weight x transfer entry, [n_y][5 i2 + k2]
 };
 using Smem = SmemT<false>;
 
 static_assert(2 * (sizeof(SmemT<false>) + 1024) <= 233472, "two CTAs must fit in the 228 KB of an SM");
 static_assert(sizeof(SmemT<true>) + 1024 <= 233472, "the energy variant must fit one CTA per SM");
+static_assert(sizeof(SmemT<false, double>) <= 232448, "the float64 tile must fit one CTA");
 
 // global node of staged node i and its mirror flags
-__device__ __forceinline__ int staged_global(const StepArgs<float>& a, int x0, int y0, int z0, int i, bool rv[3]) {
+template <typename Rs>
+__device__ __forceinline__ int staged_global(const StepArgs<Rs>& a, int x0, int y0, int z0, int i, bool rv[3]) {
   const int hx = i % S, hy = (i / S) % S, hz = i / (S * S);
   const int gx = resolve_axis(x0 - 1 + hx, a.nx, a.bc[0], rv[0]);
   const int gy = resolve_axis(y0 - 1 + hy, a.ny, a.bc[1], rv[1]);
@@ -68,41 +70,45 @@ __device__ __forceinline__ int staged_global(const StepArgs<float>& a, int x0, i
 
 // Row i of the 5-point Lagrange basis on {0, +EC1, -EC1, +EC2, -EC2}:
 // L_i(y) = D_i (y^2 - P_i)(y^2 + s_i y - Q_i), coefficients per row
-struct BasisRow {
-  float D, P, s, Q;
-  __device__ __forceinline__ explicit BasisRow(int i) {
+template <typename Rs> struct BasisRowT {
+  Rs D, P, s, Q;
+  __device__ __forceinline__ explicit BasisRowT(int i) {
     constexpr double e1s = EC1 * EC1, e2s = EC2 * EC2;
-    D = i == 0 ? float(1.0 / (e1s * e2s))
-               : (i <= 2 ? float(1.0 / (2.0 * e1s * (e1s - e2s))) : float(1.0 / (2.0 * e2s * (e2s - e1s))));
-    P = (i == 1 || i == 2) ? float(e2s) : float(e1s);
-    s = i == 1 ? float(EC1) : i == 2 ? -float(EC1) : i == 3 ? float(EC2) : i == 4 ? -float(EC2) : 0.f;
-    Q = i == 0 ? float(e2s) : 0.f;
+    D = i == 0 ? Rs(1.0 / (e1s * e2s))
+               : (i <= 2 ? Rs(1.0 / (2.0 * e1s * (e1s - e2s))) : Rs(1.0 / (2.0 * e2s * (e2s - e1s))));
+    P = (i == 1 || i == 2) ? Rs(e2s) : Rs(e1s);
+    s = i == 1 ? Rs(EC1) : i == 2 ? -Rs(EC1) : i == 3 ? Rs(EC2) : i == 4 ? -Rs(EC2) : Rs(0);
+    Q = i == 0 ? Rs(e2s) : Rs(0);
   }
-  __device__ __forceinline__ float operator()(float y) const {
-    const float y2 = y * y;
-    return D * (y2 - P) * (fmaf(s, y, y2) - Q);
+  __device__ __forceinline__ Rs operator()(Rs y) const {
+    const Rs y2 = y * y;
+    return D * (y2 - P) * (fma(s, y, y2) - Q);
   }
 };
 
 __device__ __forceinline__ double xi5(int c) { return Lattice<POND_D3Q125>::xi1(c); }
-__device__ __forceinline__ float xi5f(int c) {
-  return c == 0 ? 0.f : c == 1 ? float(EC1) : c == 2 ? -float(EC1) : c == 3 ? float(EC2) : -float(EC2);
+template <typename Rs> __device__ __forceinline__ Rs xi5r(int c) {
+  return c == 0 ? Rs(0) : c == 1 ? Rs(EC1) : c == 2 ? -Rs(EC1) : c == 3 ? Rs(EC2) : -Rs(EC2);
 }
 
 // LagrPol<3> factors of target class cls along one axis at the three stencil
 // positions coord-1, coord, coord+1 (steps.cu:151-250 fixed-origin quadratic)
-__device__ __forceinline__ void stencil_weights(int pos, double C, double U, int cls, float w[3]) {
+template <typename Rs>
+__device__ __forceinline__ void stencil_weights(int pos, double C, double U, int cls, Rs w[3]) {
   const double crd = double(pos) - (C * xi5(cls) + U);
-  lagr_weights<3, float>(crd - double(pos - 1), w);
+  lagr_weights<3, Rs>(crd - double(pos - 1), w);
 }
 
 // kE: with the energy populations of the double-distribution extension
-// (staged, transferred and contracted like f; T from their sum; one CTA per SM)
-template <bool kE>
-__global__ void __launch_bounds__(THREADS, kE ? 1 : 2) pull_d3q125_tile_kernel(StepArgs<float> a) {
+// (staged, transferred and contracted like f; T from their sum; one CTA per SM).
+// R: storage and transfer type (float64: one CTA per SM, no energy variant).
+template <bool kE, typename R = float>
+__global__ void __launch_bounds__(THREADS, (kE || sizeof(R) == 8) ? 1 : 2) pull_d3q125_tile_kernel(StepArgs<R> a) {
+  static_assert(!(kE && sizeof(R) == 8), "the float64 tile has no room for energy populations");
   using L = Lattice<POND_D3Q125>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  SmemT<kE>& sm = *reinterpret_cast<SmemT<kE>*>(smem_raw);
+  SmemT<kE, R>& sm = *reinterpret_cast<SmemT<kE, R>*>(smem_raw);
+  const R kFinMax = R(sizeof(R) == 8 ? 1.7976931348623157e308 : 3.402823466e38);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int x0 = blockIdx.x * T, y0 = blockIdx.y * T, z0 = blockIdx.z * T;
 
@@ -113,19 +119,23 @@ __global__ void __launch_bounds__(THREADS, kE ? 1 : 2) pull_d3q125_tile_kernel(S
     sm.flags[i] = (unsigned char)((rv[0] ? 1 : 0) | (rv[1] ? 2 : 0) | (rv[2] ? 4 : 0));
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-      const float v = a.g_in[(long long)k * a.N + g];
+      const R v = a.g_in[(long long)k * a.N + g];
       sm.u[k][i] = rv[k] ? -v : v;
     }
-    const float Tn = a.g_in[3 * a.N + g];
-    sm.c[i] = copysignf(sqrtf(fabsf(Tn) * float(1.0 / L::TLat)), Tn);
+    const R Tn = a.g_in[3 * a.N + g];
+    sm.c[i] = copysign(sqrt(fabs(Tn) * R(1.0 / L::TLat)), Tn);
   }
   for (int idx = tid; idx < 125 * SN; idx += THREADS) {
     const int p = idx / SN, i = idx - p * SN;
     bool rv[3];
     const int g = staged_global(a, x0, y0, z0, i, rv);
     const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(&sm.f[p * PS + i]));
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(a.f_in + (long long)p * a.N + g)
-                 : "memory");
+    if constexpr (sizeof(R) == 8)
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(a.f_in + (long long)p * a.N + g)
+                   : "memory");
+    else
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(a.f_in + (long long)p * a.N + g)
+                   : "memory");
     if constexpr (kE) {
       const unsigned dh = static_cast<unsigned>(__cvta_generic_to_shared(&sm.h[p * PS + i]));
       asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dh), "l"(a.h_in + (long long)p * a.N + g)
@@ -136,7 +146,7 @@ __global__ void __launch_bounds__(THREADS, kE ? 1 : 2) pull_d3q125_tile_kernel(S
   __syncthreads();
   for (int idx = tid; idx < 125 * SN; idx += THREADS) {
     const int p = idx / SN, i = idx - p * SN;
-    float& v = sm.f[p * PS + i];
+    R& v = sm.f[p * PS + i];
     v = finite_or_zero_f(v);
     if constexpr (kE) sm.h[p * PS + i] = finite_or_zero_f(sm.h[p * PS + i]);
   }
@@ -144,15 +154,15 @@ __global__ void __launch_bounds__(THREADS, kE ? 1 : 2) pull_d3q125_tile_kernel(S
 
   // ---- reference gauge R: the staged node at tile position (2, 2, 2)
   //      ((0, 1) if that node's gauge is not finite or its c is 0)
-  float uref[3], cref;
+  R uref[3], cref;
   {
     constexpr int ci = ((2 + 1) * S + (2 + 1)) * S + (2 + 1);
-    const float cc = sm.c[ci];
-    bool ok = fabsf(cc) <= 3.0e38f && fabsf(cc) > 1.0e-20f;
+    const R cc = sm.c[ci];
+    bool ok = fabs(cc) <= kFinMax && fabs(cc) > 1.0e-20f;
 #pragma unroll
     for (int ax = 0; ax < 3; ax++) {
       uref[ax] = sm.u[ax][ci];
-      ok = ok && fabsf(uref[ax]) <= 3.0e38f;
+      ok = ok && fabs(uref[ax]) <= kFinMax;
     }
 #pragma unroll
     for (int ax = 0; ax < 3; ax++) uref[ax] = ok ? uref[ax] : 0.f;
@@ -162,21 +172,21 @@ __global__ void __launch_bounds__(THREADS, kE ? 1 : 2) pull_d3q125_tile_kernel(S
   //      5x5 basis B[i][b] = L_i(s + r xi_b), s = (u - u_ref)/c_ref,
   //      r = +-c/c_ref; a node with a non-finite gauge contributes nothing
   {
-    const float icref = 1.f / cref;
+    const R icref = 1.f / cref;
     for (int i = tid; i < SN; i += THREADS) {
       const unsigned fl = sm.flags[i];
-      const float cn = sm.c[i];
-      bool ok = fabsf(cn) <= 3.0e38f;
-      float sq[3], rq[3];
+      const R cn = sm.c[i];
+      bool ok = fabs(cn) <= kFinMax;
+      R sq[3], rq[3];
 #pragma unroll
       for (int ax = 0; ax < 3; ax++) {
-        const float un = sm.u[ax][i];
-        ok = ok && fabsf(un) <= 3.0e38f;
+        const R un = sm.u[ax][i];
+        ok = ok && fabs(un) <= kFinMax;
         sq[ax] = (un - uref[ax]) * icref;
         rq[ax] = ((fl >> ax) & 1 ? -cn : cn) * icref;
       }
-      float* fi = sm.f + i;
-      float* hi = kE ? sm.h + i : nullptr;
+      R* fi = sm.f + i;
+      R* hi = kE ? sm.h + i : nullptr;
       if (!ok) {
         for (int pp = 0; pp < 125; pp++) fi[pp * PS] = 0.f;
         if constexpr (kE)
@@ -185,25 +195,25 @@ __global__ void __launch_bounds__(THREADS, kE ? 1 : 2) pull_d3q125_tile_kernel(S
       }
 #pragma unroll
       for (int ax = 0; ax < 3; ax++) {
-        float B[5][5];
+        R B[5][5];
 #pragma unroll
         for (int ii = 0; ii < 5; ii++) {
-          const BasisRow Li(ii);
+          const BasisRowT<R> Li(ii);
 #pragma unroll
-          for (int b = 0; b < 5; b++) B[ii][b] = finite_or_zero_f(Li(fmaf(rq[ax], xi5f(b), sq[ax])));
+          for (int b = 0; b < 5; b++) B[ii][b] = finite_or_zero_f(Li(fma(rq[ax], xi5r<R>(b), sq[ax])));
         }
         const int st = ax == 0 ? 25 : ax == 1 ? 5 : 1;
 #pragma unroll 5
         for (int o = 0; o < 25; o++) {
           const int base = ax == 0 ? o : ax == 1 ? 25 * (o / 5) + o % 5 : 5 * o;
-          float v[5], w[5];
+          R v[5], w[5];
 #pragma unroll
           for (int b = 0; b < 5; b++) v[b] = fi[(base + b * st) * PS];
 #pragma unroll
           for (int ii = 0; ii < 5; ii++) {
-            float t = B[ii][0] * v[0];
+            R t = B[ii][0] * v[0];
 #pragma unroll
-            for (int b = 1; b < 5; b++) t = fmaf(B[ii][b], v[b], t);
+            for (int b = 1; b < 5; b++) t = fma(B[ii][b], v[b], t);
             w[ii] = t;
           }
 #pragma unroll
@@ -213,9 +223,9 @@ __global__ void __launch_bounds__(THREADS, kE ? 1 : 2) pull_d3q125_tile_kernel(S
             for (int b = 0; b < 5; b++) v[b] = hi[(base + b * st) * PS];
 #pragma unroll
             for (int ii = 0; ii < 5; ii++) {
-              float t = B[ii][0] * v[0];
+              R t = B[ii][0] * v[0];
 #pragma unroll
-              for (int b = 1; b < 5; b++) t = fmaf(B[ii][b], v[b], t);
+              for (int b = 1; b < 5; b++) t = fma(B[ii][b], v[b], t);
               w[ii] = t;
             }
 #pragma unroll
@@ -239,7 +249,7 @@ __global__ void __launch_bounds__(THREADS, kE ? 1 : 2) pull_d3q125_tile_kernel(S
     if (x >= a.nx || y >= a.ny || z >= a.nz) continue;  // warp-uniform
     const long long idx = x + (long long)a.nx * (y + (long long)a.ny * z);
     // c0.load of the centre: this lane's populations (j, iy, k), iy = 0..4
-    float f0[5], h0[5];
+    R f0[5], h0[5];
 #pragma unroll
     for (int iy = 0; iy < 5; iy++) {
       f0[iy] = worker ? a.f_in[(long long)(25 * j + 5 * iy + k) * a.N + idx] : 0.f;
@@ -254,10 +264,10 @@ __global__ void __launch_bounds__(THREADS, kE ? 1 : 2) pull_d3q125_tile_kernel(S
 #pragma unroll
       for (int iy = 0; iy < 5; iy++) {
         const double w = lattice_weight_t<POND_D3Q125>(25 * j + 5 * iy + k);
-        f0[iy] = worker ? float(w) : 0.f;
+        f0[iy] = worker ? R(w) : 0.f;
         if constexpr (kE) {  // its energy at equilibrium: w (|xi|^2 + dof TLat)
           const double v2 = xi5(j) * xi5(j) + xi5(iy) * xi5(iy) + xi5(k) * xi5(k);
-          h0[iy] = worker ? float(w * (v2 + a.dof * L::TLat)) : 0.f;
+          h0[iy] = worker ? R(w * (v2 + a.dof * L::TLat)) : 0.f;
         }
       }
     }
@@ -268,24 +278,24 @@ __global__ void __launch_bounds__(THREADS, kE ? 1 : 2) pull_d3q125_tile_kernel(S
     const int qc = ((lz + 1) * S + (ly + 1)) * S + (lx + 1);  // staged centre
     int niter = 0;
     bool conv = false;
-    float acc[5], acch[5];
+    R acc[5], acch[5];
     while (niter < a.max_iter) {
       niter++;
       const double C = sqrt(Tc / L::TLat);
       // transfer R -> target per axis: G[i][k] = L_i(b + a xi_k), a = c_ref/C, b = (u_ref - U)/C
-      const float ga = float(double(cref) / C);
-      float gb[3];
+      const R ga = R(double(cref) / C);
+      R gb[3];
 #pragma unroll
-      for (int ax = 0; ax < 3; ax++) gb[ax] = float((double(uref[ax]) - U[ax]) / C);
+      for (int ax = 0; ax < 3; ax++) gb[ax] = R((double(uref[ax]) - U[ax]) / C);
       // this lane's z (class k) and x (class j) transfer rows and stencil weights
-      float tz[5], tx[5], wz[3], wx[3];
+      R tz[5], tx[5], wz[3], wx[3];
       stencil_weights(pos[2], C, U[2], k, wz);
       stencil_weights(pos[0], C, U[0], j, wx);
-      const BasisRow Lj(j), Lk(k);
+      const BasisRowT<R> Lj(j), Lk(k);
 #pragma unroll
       for (int kk = 0; kk < 5; kk++) {
-        tz[kk] = finite_or_zero_f(Lk(fmaf(ga, xi5f(kk), gb[2])));
-        tx[kk] = finite_or_zero_f(Lj(fmaf(ga, xi5f(kk), gb[0])));
+        tz[kk] = finite_or_zero_f(Lk(fma(ga, xi5r<R>(kk), gb[2])));
+        tx[kk] = finite_or_zero_f(Lj(fma(ga, xi5r<R>(kk), gb[0])));
       }
       // y coefficients of every (n_y, i2, k2): three table entries per worker lane
       __syncwarp();  // the previous iteration's readers are done with the table
@@ -293,9 +303,9 @@ __global__ void __launch_bounds__(THREADS, kE ? 1 : 2) pull_d3q125_tile_kernel(S
 #pragma unroll
         for (int r = 0; r < 3; r++) {
           const int e = 3 * lane + r, ny = e / 25, i2 = (e / 5) % 5, k2 = e % 5;
-          float wy[3];
+          R wy[3];
           stencil_weights(pos[1], C, U[1], i2, wy);
-          const float ty = finite_or_zero_f(BasisRow(i2)(fmaf(ga, xi5f(k2), gb[1])));
+          const R ty = finite_or_zero_f(BasisRowT<R>(i2)(fma(ga, xi5r<R>(k2), gb[1])));
           sm.GY[warp][ny][5 * i2 + k2] = (ny == 0 ? wy[0] : ny == 1 ? wy[1] : wy[2]) * ty;
         }
       }
@@ -304,47 +314,47 @@ __global__ void __launch_bounds__(THREADS, kE ? 1 : 2) pull_d3q125_tile_kernel(S
       for (int iy = 0; iy < 5; iy++) { acc[iy] = 0.f; acch[iy] = 0.f; }
 #pragma unroll
       for (int nx = 0; nx < 3; nx++) {
-        float Yr[5] = {0.f, 0.f, 0.f, 0.f, 0.f};  // (j, i2, k) of the row
-        float Yh[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+        R Yr[5] = {0.f, 0.f, 0.f, 0.f, 0.f};  // (j, i2, k) of the row
+        R Yh[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll 1
         for (int ny = 0; ny < 3; ny++) {
-          float Zc[5] = {0.f, 0.f, 0.f, 0.f, 0.f};  // (j, k2, k) of the column
-          float Zh[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+          R Zc[5] = {0.f, 0.f, 0.f, 0.f, 0.f};  // (j, k2, k) of the column
+          R Zh[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll 1
           for (int nz = 0; nz < 3; nz++) {
-            const float wn = nz == 0 ? wz[0] : nz == 1 ? wz[1] : wz[2];
-            float gz[5];
+            const R wn = nz == 0 ? wz[0] : nz == 1 ? wz[1] : wz[2];
+            R gz[5];
 #pragma unroll
             for (int k3 = 0; k3 < 5; k3++) gz[k3] = wn * tz[k3];
-            const float* fq = sm.f + (25 * j) * PS + qc + (nz - 1) * S * S + (ny - 1) * S + (nx - 1);
+            const R* fq = sm.f + (25 * j) * PS + qc + (nz - 1) * S * S + (ny - 1) * S + (nx - 1);
 #pragma unroll
             for (int k2 = 0; k2 < 5; k2++)
 #pragma unroll
-              for (int k3 = 0; k3 < 5; k3++) Zc[k2] = fmaf(gz[k3], fq[(5 * k2 + k3) * PS], Zc[k2]);
+              for (int k3 = 0; k3 < 5; k3++) Zc[k2] = fma(gz[k3], fq[(5 * k2 + k3) * PS], Zc[k2]);
             if constexpr (kE) {
-              const float* hq = sm.h + (fq - sm.f);
+              const R* hq = sm.h + (fq - sm.f);
 #pragma unroll
               for (int k2 = 0; k2 < 5; k2++)
 #pragma unroll
-                for (int k3 = 0; k3 < 5; k3++) Zh[k2] = fmaf(gz[k3], hq[(5 * k2 + k3) * PS], Zh[k2]);
+                for (int k3 = 0; k3 < 5; k3++) Zh[k2] = fma(gz[k3], hq[(5 * k2 + k3) * PS], Zh[k2]);
             }
           }
-          const float* gy = sm.GY[warp][ny];
+          const R* gy = sm.GY[warp][ny];
 #pragma unroll
           for (int i2 = 0; i2 < 5; i2++)
 #pragma unroll
             for (int k2 = 0; k2 < 5; k2++) {
-              Yr[i2] = fmaf(gy[5 * i2 + k2], Zc[k2], Yr[i2]);
-              if constexpr (kE) Yh[i2] = fmaf(gy[5 * i2 + k2], Zh[k2], Yh[i2]);
+              Yr[i2] = fma(gy[5 * i2 + k2], Zc[k2], Yr[i2]);
+              if constexpr (kE) Yh[i2] = fma(gy[5 * i2 + k2], Zh[k2], Yh[i2]);
             }
         }
 #pragma unroll
         for (int k1 = 0; k1 < 5; k1++) {
-          const float g = wx[nx] * tx[k1];
+          const R g = wx[nx] * tx[k1];
 #pragma unroll
           for (int i2 = 0; i2 < 5; i2++) {
-            acc[i2] = fmaf(g, __shfl_sync(0xffffffffu, Yr[i2], 5 * k1 + k), acc[i2]);
-            if constexpr (kE) acch[i2] = fmaf(g, __shfl_sync(0xffffffffu, Yh[i2], 5 * k1 + k), acch[i2]);
+            acc[i2] = fma(g, __shfl_sync(0xffffffffu, Yr[i2], 5 * k1 + k), acc[i2]);
+            if constexpr (kE) acch[i2] = fma(g, __shfl_sync(0xffffffffu, Yh[i2], 5 * k1 + k), acch[i2]);
           }
         }
       }
@@ -402,23 +412,23 @@ __global__ void __launch_bounds__(THREADS, kE ? 1 : 2) pull_d3q125_tile_kernel(S
       if (all_ok) { conv = true; break; }
     }
     // BGK and store (steps.cu:230-248)
-    const float rr = float(rho0), dtau = float(a.dtau);
+    const R rr = R(rho0), dtau = R(a.dtau);
     if (worker)
 #pragma unroll
       for (int iy = 0; iy < 5; iy++) {
         const int p = 25 * j + 5 * iy + k;
-        const float fb = f0[iy] + dtau * (rr * float(lattice_weight_t<POND_D3Q125>(p)) - f0[iy]);
+        const R fb = f0[iy] + dtau * (rr * R(lattice_weight_t<POND_D3Q125>(p)) - f0[iy]);
         a.f_out[(long long)p * a.N + idx] = fb;
         if constexpr (kE) {  // h toward rho w (|v|^2 + dof T) in the final gauge
           const double Cf = sqrt(fabs(Tc) * (1.0 / L::TLat));
           const double vx = Cf * xi5(j) + U[0], vy = Cf * xi5(iy) + U[1], vz = Cf * xi5(k) + U[2];
-          const float heq = float(double(rr) * lattice_weight_t<POND_D3Q125>(p) *
+          const R heq = R(double(rr) * lattice_weight_t<POND_D3Q125>(p) *
                                   (vx * vx + vy * vy + vz * vz + a.dof * Tc));
           a.h_out[(long long)p * a.N + idx] = h0[iy] + dtau * (heq - h0[iy]);
         }
       }
     if (lane == 0) {
-      const float u0 = float(U[0]), u1 = float(U[1]), u2 = float(U[2]), ts = float(Tc);
+      const R u0 = R(U[0]), u1 = R(U[1]), u2 = R(U[2]), ts = R(Tc);
       a.rho_out[idx] = rr;
       a.g_out[idx] = u0; a.g_out[a.N + idx] = u1; a.g_out[2 * a.N + idx] = u2; a.g_out[3 * a.N + idx] = ts;
       if (a.niter_out) a.niter_out[idx] = niter;
