@@ -23,6 +23,42 @@ __device__ __forceinline__ double minmod_d(double a, double b) {  // steps.cu:11
   return b;
 }
 
+// steps.cu:447 with FluxTVDdif (:118-124): the cubic value at x minus the
+// minmod-limited flux difference, from the slots F(x-2v), F(x-v), F(x), F(x+v)
+__device__ __forceinline__ double tvd_combine(double Fm2, double Fm1, double F0, double Fp1, double v) {
+  const int sg = (0.0 < v) - (v < 0.0);
+  const double flux = F0 - Fm1 + sg * 0.5 * minmod_d(F0 - Fm1, Fp1 - F0) - sg * 0.5 * minmod_d(F0 - Fm1, Fm1 - Fm2);
+  return F0 - flux;
+}
+
+// steps.cu:774-825 propagateWENO<3,5>: three quadratic candidates on the five
+// transformed values u[0..4] at round(crd)-2 .. round(crd)+2, Jiang-Shu
+// smoothness indicators, eps = 1e-6
+__device__ __forceinline__ double weno5_combine(const double u[5], double crd) {
+  const double u1 = u[0], u2 = u[1], u3 = u[2], u4 = u[3], u5 = u[4];
+  const double fx = floor(crd + 0.5);
+  double S[3];
+#pragma unroll
+  for (int j = 0; j < 3; j++) {  // LagrEval<3> with origins fx-2, fx-1, fx
+    double w3[3];
+    lagr_weights<3, double>(crd - (fx - 2 + j), w3);
+    S[j] = w3[0] * u[j] + w3[1] * u[j + 1] + w3[2] * u[j + 2];
+  }
+  const double cd = crd - (int)fx;
+  const double d0 = (cd * cd - 3 * cd + 2) / 12.;
+  const double d2 = (cd * cd + 3 * cd + 2) / 12.;
+  const double d1 = 1. - d0 - d2;
+  const double b0 = (10 * u3 * u3 + (11 * u1 - 31 * u2) * u3 + 25 * u2 * u2 - 19 * u1 * u2 + 4 * u1 * u1) / 3.0;
+  const double b1 = (4 * u4 * u4 + (5 * u2 - 13 * u3) * u4 + 13 * u3 * u3 - 13 * u2 * u3 + 4 * u2 * u2) / 3.0;
+  const double b2 = (4 * u5 * u5 + (11 * u3 - 19 * u4) * u5 + 25 * u4 * u4 - 31 * u3 * u4 + 10 * u3 * u3) / 3.0;
+  double w0 = d0 / ((1e-6 + b0) * (1e-6 + b0));
+  double w1 = d1 / ((1e-6 + b1) * (1e-6 + b1));
+  double w2 = d2 / ((1e-6 + b2) * (1e-6 + b2));
+  const double ws = w0 + w1 + w2;
+  w0 /= ws; w1 /= ws; w2 /= ws;
+  return w0 * S[0] + w1 * S[1] + w2 * S[2];
+}
+
 template <int SCHEME, typename R>
 __global__ void __launch_bounds__(128) pull_1d_scheme_kernel(StepArgs<R> a) {
   using L = Lattice<POND_D1Q5>;
@@ -103,37 +139,11 @@ __global__ void __launch_bounds__(128) pull_1d_scheme_kernel(StepArgs<R> a) {
       R fnew[Q];
 #pragma unroll
       for (int k = 0; k < Q; k++) {
-        if (SCHEME == POND_TVD) {
-          const double Fm2 = acc[k][0], Fm1 = acc[k][1], F0 = acc[k][2], Fp1 = acc[k][3];
-          const int sg = (0.0 < vk[k]) - (vk[k] < 0.0);
-          const double flux = F0 - Fm1 + sg * 0.5 * minmod_d(F0 - Fm1, Fp1 - F0) -
-                              sg * 0.5 * minmod_d(F0 - Fm1, Fm1 - Fm2);
-          fnew[k] = R(F0 - flux);
+        if constexpr (SCHEME == POND_TVD) {
+          fnew[k] = R(tvd_combine(acc[k][0], acc[k][1], acc[k][2], acc[k][3], vk[k]));
         } else {
-          const double u1 = acc[k][0], u2 = acc[k][1], u3 = acc[k][2], u4 = acc[k][3], u5 = acc[k][4];
-          const double crd = double(x) - vk[k];
-          const double fx = floor(crd + 0.5);
-          double S[3];
-#pragma unroll
-          for (int j = 0; j < 3; j++) {  // LagrEval<3> with origins fx-2, fx-1, fx
-            double w3[3];
-            lagr_weights<3, double>(crd - (fx - 2 + j), w3);
-            const double uu[5] = {u1, u2, u3, u4, u5};
-            S[j] = w3[0] * uu[j] + w3[1] * uu[j + 1] + w3[2] * uu[j + 2];
-          }
-          const double cd = crd - (int)fx;
-          const double d0 = (cd * cd - 3 * cd + 2) / 12.;
-          const double d2 = (cd * cd + 3 * cd + 2) / 12.;
-          const double d1 = 1. - d0 - d2;
-          const double b0 = (10 * u3 * u3 + (11 * u1 - 31 * u2) * u3 + 25 * u2 * u2 - 19 * u1 * u2 + 4 * u1 * u1) / 3.0;
-          const double b1 = (4 * u4 * u4 + (5 * u2 - 13 * u3) * u4 + 13 * u3 * u3 - 13 * u2 * u3 + 4 * u2 * u2) / 3.0;
-          const double b2 = (4 * u5 * u5 + (11 * u3 - 19 * u4) * u5 + 25 * u4 * u4 - 31 * u3 * u4 + 10 * u3 * u3) / 3.0;
-          double w0 = d0 / ((1e-6 + b0) * (1e-6 + b0));
-          double w1 = d1 / ((1e-6 + b1) * (1e-6 + b1));
-          double w2 = d2 / ((1e-6 + b2) * (1e-6 + b2));
-          const double ws = w0 + w1 + w2;
-          w0 /= ws; w1 /= ws; w2 /= ws;
-          fnew[k] = R(w0 * S[0] + w1 * S[1] + w2 * S[2]);
+          const double uu[5] = {acc[k][0], acc[k][1], acc[k][2], acc[k][3], acc[k][4]};
+          fnew[k] = R(weno5_combine(uu, double(x) - vk[k]));
         }
       }
       if (moments_and_test<POND_D1Q5, R>(a, fnew, f0, C, rho0, U, T)) { conv = true; break; }

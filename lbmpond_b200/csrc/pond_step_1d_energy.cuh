@@ -141,39 +141,13 @@ __global__ void __launch_bounds__(128) pull_1d_energy_kernel(StepArgs<R> a) {
         for (int k = 0; k < Q; k++) {
           const R* sl = e == 0 ? accf[k] : acch[k];
           double val;
-          if (kLagr) {
+          if constexpr (kLagr) {
             val = sl[0];
-          } else if (SCHEME == POND_TVD) {  // steps.cu:447 with FluxTVDdif (:118-124)
-            const double Fm2 = sl[0], Fm1 = sl[1], F0 = sl[2], Fp1 = sl[3];
-            const int sg = (0.0 < vk[k]) - (vk[k] < 0.0);
-            const double flux = F0 - Fm1 + sg * 0.5 * minmod_d(F0 - Fm1, Fp1 - F0) -
-                                sg * 0.5 * minmod_d(F0 - Fm1, Fm1 - Fm2);
-            val = F0 - flux;
-          } else {  // steps.cu:774-825
-            const double u1 = sl[0], u2 = sl[1], u3 = sl[2], u4 = sl[3], u5 = sl[4];
-            const double crd = double(x) - vk[k];
-            const double fx = floor(crd + 0.5);
-            double S[3];
-#pragma unroll
-            for (int j = 0; j < 3; j++) {
-              double w3[3];
-              lagr_weights<3, double>(crd - (fx - 2 + j), w3);
-              const double uu[5] = {u1, u2, u3, u4, u5};
-              S[j] = w3[0] * uu[j] + w3[1] * uu[j + 1] + w3[2] * uu[j + 2];
-            }
-            const double cd = crd - (int)fx;
-            const double d0 = (cd * cd - 3 * cd + 2) / 12.;
-            const double d2 = (cd * cd + 3 * cd + 2) / 12.;
-            const double d1 = 1. - d0 - d2;
-            const double b0 = (10 * u3 * u3 + (11 * u1 - 31 * u2) * u3 + 25 * u2 * u2 - 19 * u1 * u2 + 4 * u1 * u1) / 3.0;
-            const double b1 = (4 * u4 * u4 + (5 * u2 - 13 * u3) * u4 + 13 * u3 * u3 - 13 * u2 * u3 + 4 * u2 * u2) / 3.0;
-            const double b2 = (4 * u5 * u5 + (11 * u3 - 19 * u4) * u5 + 25 * u4 * u4 - 31 * u3 * u4 + 10 * u3 * u3) / 3.0;
-            double w0 = d0 / ((1e-6 + b0) * (1e-6 + b0));
-            double w1 = d1 / ((1e-6 + b1) * (1e-6 + b1));
-            double w2 = d2 / ((1e-6 + b2) * (1e-6 + b2));
-            const double ws = w0 + w1 + w2;
-            w0 /= ws; w1 /= ws; w2 /= ws;
-            val = w0 * S[0] + w1 * S[1] + w2 * S[2];
+          } else if constexpr (SCHEME == POND_TVD) {
+            val = tvd_combine(sl[0], sl[1], sl[2], sl[3], vk[k]);
+          } else {
+            const double uu[5] = {sl[0], sl[1], sl[2], sl[3], sl[4]};
+            val = weno5_combine(uu, double(x) - vk[k]);
           }
           if (e == 0) fnew[k] = R(val); else hnew[k] = R(val);
         }
