@@ -116,6 +116,10 @@ class Batch:
         if every and (X is None or Y is None or X.shape[0] != Y.shape[0]):
             raise ValueError("X and Y must be given with the same row count")
         cap = X.shape[0] if X is not None else 0
+        for t in (X, Y):  # torch's queued work on the buffers ends before the library writes them
+            if t is not None and t.is_cuda:
+                import torch
+                torch.cuda.current_stream(t.device).synchronize()
         _lib.check(self._L.pond_batch_set_pairs(self._h, X.data_ptr() if X is not None else None,
                                                 Y.data_ptr() if Y is not None else None, int(cap), int(every),
                                                 int(stride)))

@@ -16,6 +16,19 @@ from . import _lib
 NIN, NOUT = 39, 4
 
 
+def _torch_idle(*tensors):
+    """Wait for torch's queued work on the tensors' devices.  The library runs
+    on its own streams: a tensor torch has just written (or a block its
+    caching allocator has just handed back while a kernel still reads it)
+    must be settled before the library reads or writes that memory.  Every
+    library call synchronises its own stream before returning, so the other
+    direction needs nothing."""
+    import torch
+    for t in tensors:
+        if t is not None and t.is_cuda:
+            torch.cuda.current_stream(t.device).synchronize()
+
+
 class Predictor:
     def __init__(self, hidden=64, seed=0, device=0):
         L = _lib.load()
@@ -67,10 +80,12 @@ class Predictor:
 
     # -- training (X, Y: torch float32 CUDA tensors [n, 35], [n, 4])
     def fit_stats(self, X, Y):
+        _torch_idle(X, Y)
         _lib.check(self._L.pond_mlp_fit_stats(self._h, X.data_ptr(), Y.data_ptr(), X.shape[0]))
 
     def train(self, X, Y, steps=1000, batch=4096, lr=2e-3):
         loss = np.empty(steps, np.float32)
+        _torch_idle(X, Y)
         _lib.check(self._L.pond_mlp_train(self._h, X.data_ptr(), Y.data_ptr(), X.shape[0], int(batch), int(steps),
                                           float(lr), loss.ctypes.data))
         return loss
@@ -78,6 +93,7 @@ class Predictor:
     def gradients(self, X, Y):
         g = np.empty(self.nparams, np.float32)
         loss = np.empty(1, np.float32)
+        _torch_idle(X, Y)
         _lib.check(self._L.pond_mlp_gradients(self._h, X.data_ptr(), Y.data_ptr(), X.shape[0], g.ctypes.data,
                                               loss.ctypes.data))
         return float(loss[0]), g
@@ -86,6 +102,7 @@ class Predictor:
         import torch
         if out is None:
             out = torch.empty((X.shape[0], NOUT), dtype=torch.float32, device=X.device)
+        _torch_idle(X, out)
         _lib.check(self._L.pond_mlp_forward(self._h, X.data_ptr(), out.data_ptr(), X.shape[0]))
         return out
 
@@ -108,6 +125,7 @@ def collect_pairs(solver, X, Y, offset_rows=0, stride=7, seed=0, nodes=None):
     xp = X.data_ptr() + offset_rows * NIN * 4
     yp = Y.data_ptr() + offset_rows * NOUT * 4
     np_ = nodes_all.data_ptr() + base * 8
+    _torch_idle(X, Y, nodes_all)
     _lib.check(L.pond_collect_pairs(solver.handle, xp, yp, np_, int(cap), int(stride), int(seed), ctypes.byref(n)))
     n = int(n.value)
     if n > 1:  # the kernel appends rows in arrival order: sort them by node, then shuffle with the seed
