@@ -636,7 +636,7 @@ def main():
     ap.add_argument("--ref-size", type=int, default=24)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--ref-cuda", action="store_true", help="also time the reference's own kernels (64^3)")
+    ap.add_argument("--ref-cuda", action="store_true", help="with --impl reference: also time the reference's own kernels (64^3)")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched 1D measurement")
     ap.add_argument("--batch-steps", type=int, default=1000)
     ap.add_argument("--batch-problems", type=int, default=4096)
@@ -651,7 +651,10 @@ def main():
         world = int(os.environ.get("WORLD_SIZE", "1"))
         if rank != 0:
             return
-        print(json.dumps(run_reference(args, rank, world)), flush=True)
+        out = run_reference(args, rank, world)
+        if args.ref_cuda:
+            out["reference_cuda"] = reference_cuda()
+        print(json.dumps(out), flush=True)
         return
     if args.workload == "batch1d":
         rank, local, world, pg = dist_setup(args.gpus)
@@ -670,8 +673,6 @@ def main():
     out = run_ours(args, rank, local, world, pg)
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(args.spinup)
-    if rank == 0 and args.ref_cuda:
-        out["reference_cuda"] = reference_cuda()
     if rank == 0 and world == 1 and not args.no_batch:
         out["batch1d"] = run_batch1d(args.batch_steps, args.batch_problems)
     if pg is not None:

@@ -124,7 +124,7 @@ def load(path: str | None = None):
         return _lib
     path = path or LIB_PATH
     if not os.path.exists(path):
-        raise ImportError(f"{path} is missing: run `python -m lbmpond_b200.build` (or __graft_entry__.build())")
+        raise ImportError(f"{path} is missing: run `python -m lbmpond_b200.build`")
     L = ctypes.CDLL(path)
     for name, (res, args) in SIGNATURES.items():
         fn = getattr(L, name)
