@@ -51,7 +51,12 @@ enum {
   POND_LAGR2 = 2, POND_LAGR3 = 3, POND_LAGR4 = 4, POND_LAGR5 = 5, /* propagate<N>, steps.cu:986 */
   POND_FIXED3 = 6, /* quadratic, origin fixed at coord-1: PonDstepD3Q125 steps.cu:151 */
   POND_TVD = 7,    /* flux-difference minmod form, steps.cu:118-124 with call site :447 */
-  POND_WENO5 = 8   /* propagateWENO<3,5>, steps.cu:774-825 */
+  POND_WENO5 = 8,  /* propagateWENO<3,5>, steps.cu:774-825 */
+  /* one-dimensional meshes (D1Q5, Ny = Nz = 1, periodic), with a node mask: */
+  POND_GAP2 = 9,        /* linear between the nearest active nodes, propagate_nonequal_1D<2>,
+                           steps.cu:1122-1149 (call site :449) */
+  POND_NONUNIFORM3 = 10 /* quadratic Lagrange on the node positions of x-1, x, x+1,
+                           propagateNR_1D + LagrPolNR_1D, steps.cu:882-908,590-594 (call site :453) */
 };
 /* boundaries per axis: periodic is the reference (steps.cu:1015-1017); mirror
    is its disabled outflow reflection (steps.cu:1004-1013); clamp = zero gradient */
@@ -167,6 +172,47 @@ int pond_copy_state(pond_ctx* dst, pond_ctx* src);
    operations of its basis contractions (a multiply-add counts 2), for the
    other kernels the stencil nodes transformed */
 int pond_last_step_work(pond_ctx* ctx, int64_t* work);
+
+/* ---- one-dimensional mesh: node mask, AMR, node positions -------------
+   A context made with POND_GAP2 or POND_NONUNIFORM3 owns a node mask (the
+   reference's Cinfo::set, structs.cuh:90-95; all nodes active after
+   pond_create, init.cu:106).  The step skips inactive nodes (steps.cu:359)
+   and carries them over unchanged; diagnostics sum active nodes only
+   (update.cu:56-69).  A POND_NONUNIFORM3 context also owns node positions
+   (Cell::p.x under NRMESH, structs.cuh:40-42; p_x = x after pond_create,
+   init.cu:100-103) and weights the diagnostics by half the distance between
+   each node's neighbours (update.cu:59-62). */
+/* mask[N] bytes, nonzero = active */
+int pond_set_mask(pond_ctx* ctx, const uint8_t* mask);
+int pond_get_mask(pond_ctx* ctx, uint8_t* mask);
+/* positions[N]: finite, strictly increasing, last - first < Nx (node units) */
+int pond_set_positions(pond_ctx* ctx, const double* positions);
+int pond_get_positions(pond_ctx* ctx, double* positions);
+/* AMR_add (amr.cu:1-27, with cinfo_setnew_reset / cinfo_set_new of
+   update.cu:30-39) on the current state: every active node whose next active
+   node (periodic) differs from it by (du_x)^2 / min(T) > tol or
+   |1 - rho/rho_next| > tol activates the midpoint of an even gap between
+   them, holding the average of the two records in both time levels (the
+   reference's tol is 0.01).  *added = nodes activated; *limit_hits = nodes
+   over the threshold with an adjacent neighbour (the reference prints
+   "limit of cells division exceeded").  Either output may be NULL. */
+int pond_amr_refine(pond_ctx* ctx, double tol, int64_t* added, int64_t* limit_hits);
+/* AMR_remove (amr.cu:28-56): deactivates, in one pass in node order over
+   the mask as it changes, each active node whose nearest active neighbours
+   are both within 3 nodes and within tol in (du_x)^2 / T and density ratio.
+   The result equals the reference's serial pass; it is computed as a
+   parallel prefix over the pass's 8-state automaton. */
+int pond_amr_coarsen(pond_ctx* ctx, double tol, int64_t* removed);
+
+/* ---- time-step rescaling (TimeCorr, update.cu:15-28) ------------------
+   Multiplies every node's u by s and T by s*s in the current state (lattice
+   velocities are displacements per step) and the context's dt by s; any
+   lattice.  pond_set_dt_adapt applies the reference's disabled policy after
+   every step (update.cu:116-119): s = 1/2 when the step's NiterMax >= niter_hi,
+   s = 2 when it is <= niter_lo (the reference's values: 1000 and 4); on = 0
+   turns it off.  The step's diagnostics are rescaled with the state. */
+int pond_rescale_time(pond_ctx* ctx, double s);
+int pond_set_dt_adapt(pond_ctx* ctx, int on, int niter_hi, int niter_lo);
 
 /* ---- learned starting gauge ------------------------------------------
    A small network (39 -> H -> H -> 4, tanh, H = 64 or 128; BF16 tensor-core

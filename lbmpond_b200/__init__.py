@@ -22,12 +22,13 @@ import os
 import numpy as np
 
 from . import _lib
-from ._lib import (BC_CLAMP, BC_MIRROR, BC_PERIODIC, D1Q5, D3Q27, D3Q125, FIXED3, FP32, FP64, IC_ACOUSTIC,
-                   IC_SOD_X, IC_SPHERE, IC_TGV, IC_UNIFORM, LAGR2, LAGR3, LAGR4, LAGR5, TVD, WENO5, PondError)
+from ._lib import (BC_CLAMP, BC_MIRROR, BC_PERIODIC, D1Q5, D3Q27, D3Q125, FIXED3, FP32, FP64, GAP2, IC_ACOUSTIC,
+                   IC_SOD_X, IC_SPHERE, IC_TGV, IC_UNIFORM, LAGR2, LAGR3, LAGR4, LAGR5, NONUNIFORM3, TVD, WENO5,
+                   PondError)
 
 __all__ = ["Solver", "PondError", "lattice_q", "D1Q5", "D3Q27", "D3Q125", "LAGR2", "LAGR3", "LAGR4", "LAGR5",
-           "FIXED3", "TVD", "WENO5", "BC_PERIODIC", "BC_CLAMP", "BC_MIRROR", "FP32", "FP64", "IC_ACOUSTIC",
-           "IC_SOD_X", "IC_SPHERE", "IC_TGV", "IC_UNIFORM", "write_arr", "read_arr"]
+           "FIXED3", "TVD", "WENO5", "GAP2", "NONUNIFORM3", "BC_PERIODIC", "BC_CLAMP", "BC_MIRROR", "FP32", "FP64",
+           "IC_ACOUSTIC", "IC_SOD_X", "IC_SPHERE", "IC_TGV", "IC_UNIFORM", "write_arr", "read_arr"]
 
 _LATTICES = {"D1Q5": D1Q5, "D3Q27": D3Q27, "D3Q125": D3Q125}
 _BCS = {"periodic": BC_PERIODIC, "clamp": BC_CLAMP, "zero_gradient": BC_CLAMP, "mirror": BC_MIRROR}
@@ -151,6 +152,54 @@ class Solver:
         return {"mass": d.mass, "moment": tuple(d.moment), "enrg": d.enrg, "k": d.k, "niter_max": d.niter_max,
                 "niter_mean": d.niter_mean, "niter_sum": d.niter_sum, "nonconverged": d.nonconverged,
                 "istep": d.istep, "curtime": d.curtime}
+
+    # -- one-dimensional mesh (GAP2 / NONUNIFORM3): node mask, AMR, node positions
+    def set_mask(self, mask):
+        """Node mask (Cinfo::set): nonzero = active; inactive nodes are skipped by the step."""
+        m = np.ascontiguousarray(mask, dtype=np.uint8).reshape(self.N)
+        _lib.check(self._L.pond_set_mask(self._ctx, m.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))))
+
+    def get_mask(self):
+        m = np.empty(self.N, dtype=np.uint8)
+        _lib.check(self._L.pond_get_mask(self._ctx, m.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))))
+        return m
+
+    def set_positions(self, x):
+        """Node positions (Cell::p.x) of a NONUNIFORM3 context: increasing, spanning less than Nx."""
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(self.N)
+        _lib.check(self._L.pond_set_positions(self._ctx, _dp(x)))
+
+    def get_positions(self):
+        x = np.empty(self.N)
+        _lib.check(self._L.pond_get_positions(self._ctx, _dp(x)))
+        return x
+
+    def amr_refine(self, tol=0.01):
+        """AMR_add (amr.cu:1-27) on the current state; returns (added, limit_hits)."""
+        a, h = ctypes.c_int64(), ctypes.c_int64()
+        _lib.check(self._L.pond_amr_refine(self._ctx, float(tol), ctypes.byref(a), ctypes.byref(h)))
+        return int(a.value), int(h.value)
+
+    def amr_coarsen(self, tol=0.01):
+        """AMR_remove (amr.cu:28-56) on the current state; returns the nodes removed."""
+        r = ctypes.c_int64()
+        _lib.check(self._L.pond_amr_coarsen(self._ctx, float(tol), ctypes.byref(r)))
+        return int(r.value)
+
+    # -- time-step rescaling (TimeCorr)
+    def rescale_time(self, s):
+        """u *= s, T *= s*s in the current state and dt *= s (update.cu:15-28)."""
+        _lib.check(self._L.pond_rescale_time(self._ctx, float(s)))
+
+    def set_dt_adapt(self, on=True, niter_hi=1000, niter_lo=4):
+        """After every step: dt halves when NiterMax >= niter_hi, doubles when <= niter_lo (update.cu:116-119)."""
+        _lib.check(self._L.pond_set_dt_adapt(self._ctx, 1 if on else 0, int(niter_hi), int(niter_lo)))
+
+    @property
+    def dt(self) -> float:
+        p = _lib.PondParams()
+        _lib.check(self._L.pond_get_params(self._ctx, ctypes.byref(p)))
+        return float(p.dt)
 
     def keep_niter(self, on=True):
         _lib.check(self._L.pond_keep_niter(self._ctx, 1 if on else 0))

@@ -14,7 +14,7 @@ STATUS = {
 }
 
 D1Q5, D3Q27, D3Q125 = 0, 1, 2
-LAGR2, LAGR3, LAGR4, LAGR5, FIXED3, TVD, WENO5 = 2, 3, 4, 5, 6, 7, 8
+LAGR2, LAGR3, LAGR4, LAGR5, FIXED3, TVD, WENO5, GAP2, NONUNIFORM3 = 2, 3, 4, 5, 6, 7, 8, 9, 10
 BC_PERIODIC, BC_CLAMP, BC_MIRROR = 0, 1, 2
 FP32, FP64 = 0, 1
 IC_ACOUSTIC, IC_SOD_X, IC_SPHERE, IC_TGV, IC_UNIFORM = 0, 1, 2, 3, 4
@@ -46,6 +46,8 @@ class PondDiag(ctypes.Structure):
 _vp = ctypes.c_void_p
 _dp = ctypes.POINTER(ctypes.c_double)
 _i32p = ctypes.POINTER(ctypes.c_int32)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_u8p = ctypes.POINTER(ctypes.c_uint8)
 SIGNATURES = {
     "pond_abi_version": (ctypes.c_int, []),
     "pond_status_string": (ctypes.c_char_p, [ctypes.c_int]),
@@ -74,6 +76,14 @@ SIGNATURES = {
     "pond_last_step_work": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int64)]),
     "pond_copy_state": (ctypes.c_int, [_vp, _vp]),
     "pond_step_noalloc": (ctypes.c_int, [ctypes.POINTER(PondParams)] + [_vp] * 8),
+    "pond_set_mask": (ctypes.c_int, [_vp, _u8p]),
+    "pond_get_mask": (ctypes.c_int, [_vp, _u8p]),
+    "pond_set_positions": (ctypes.c_int, [_vp, _dp]),
+    "pond_get_positions": (ctypes.c_int, [_vp, _dp]),
+    "pond_amr_refine": (ctypes.c_int, [_vp, ctypes.c_double, _i64p, _i64p]),
+    "pond_amr_coarsen": (ctypes.c_int, [_vp, ctypes.c_double, _i64p]),
+    "pond_rescale_time": (ctypes.c_int, [_vp, ctypes.c_double]),
+    "pond_set_dt_adapt": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "pond_mlp_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(_vp)]),
     "pond_mlp_destroy": (ctypes.c_int, [_vp]),
     "pond_mlp_num_params": (ctypes.c_int, [_vp]),

@@ -61,7 +61,9 @@ double lattice_dim(int lattice) { return lattice == POND_D1Q5 ? 1.0 : 3.0; }
 
 bool scheme_supported(int lattice, int interp) {
   switch (lattice) {
-    case POND_D1Q5: return (interp >= POND_LAGR2 && interp <= POND_LAGR5) || interp == POND_TVD || interp == POND_WENO5;
+    case POND_D1Q5:
+      return (interp >= POND_LAGR2 && interp <= POND_LAGR5) || interp == POND_TVD || interp == POND_WENO5 ||
+             interp == POND_GAP2 || interp == POND_NONUNIFORM3;
     case POND_D3Q27: return interp >= POND_LAGR2 && interp <= POND_LAGR5;
     case POND_D3Q125: return interp == POND_FIXED3;
     default: return false;
@@ -223,6 +225,11 @@ int pond_create(const pond_params* p, pond_ctx** out) {
   if (!(p->tol_abs >= 0) || !(p->tol_rel >= 0)) return set_error(POND_ERR_ARG, "tolerances must be >= 0");
   if (p->lattice == POND_D1Q5 && (p->interp == POND_TVD || p->interp == POND_WENO5) && (p->Ny != 1 || p->Nz != 1))
     return set_error(POND_ERR_UNSUPPORTED, "TVD/WENO5 run on 1D grids (Ny = Nz = 1)");
+  if (p->lattice == POND_D1Q5 && mesh_scheme(p->interp)) {
+    if (p->Ny != 1 || p->Nz != 1 || p->Nx < 3) return set_error(POND_ERR_UNSUPPORTED, "mesh schemes run on 1D grids, Nx >= 3");
+    if (p->bc[0] != POND_BC_PERIODIC) return set_error(POND_ERR_UNSUPPORTED, "mesh schemes are periodic");
+    if (p->ddf || p->learned) return set_error(POND_ERR_UNSUPPORTED, "mesh schemes carry neither energy populations nor the learned start");
+  }
   if (p->ddf != 0 && p->ddf != 1) return set_error(POND_ERR_ARG, "ddf must be 0 or 1");
   if (p->ddf) {
     const bool d1 = p->lattice == POND_D1Q5 && p->Ny == 1 && p->Nz == 1;
@@ -483,6 +490,10 @@ int pond_step(pond_ctx* c, int nsteps) {
     c->cur = 1 - c->cur;  // LBMParamsHost::swapLS (structs.cuh:148)
     c->istep++;
     c->curtime += c->p.dt;
+    if (c->dt_adapt) {  // update.cu:116-119, after curtime advanced by the old dt
+      st = dt_adapt_after_step(c);
+      if (st != POND_OK) return st;
+    }
   }
   e = cudaEventRecord(c->ev1, c->stream);
   if (e != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
@@ -576,6 +587,15 @@ int pond_copy_state(pond_ctx* dst, pond_ctx* src) {
   }
   e = cudaStreamSynchronize(dst->stream);
   if (e != cudaSuccess) return cuda_fail(e, "pond_copy_state");
+  if (dst->mask[0] && src->mask[0]) {  // the mesh of the source goes with its state
+    e = cudaMemcpyAsync(dst->mask[dst->mask_cur], src->mask[src->mask_cur], (size_t)dst->N, cudaMemcpyDeviceToDevice,
+                        dst->stream);
+    if (e == cudaSuccess && dst->pos && src->pos)
+      e = cudaMemcpyAsync(dst->pos, src->pos, (size_t)dst->N * sizeof(double), cudaMemcpyDeviceToDevice, dst->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(dst->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pond_copy_state");
+    dst->n_active = src->n_active;
+  }
   dst->initialized = true;
   dst->have_sums = false;
   dst->istep = src->istep;
@@ -608,7 +628,8 @@ int pond_diagnostics(pond_ctx* c, pond_diag* out) {
     out->k = s.k;
     out->niter_max = s.niter_max;
     out->niter_sum = (int64_t)s.niter_sum;
-    out->niter_mean = c->N ? double(s.niter_sum) / double(c->N) : 0.0;
+    const long long nodes = c->mask[0] ? c->n_active : c->N;  // nodes the step visited
+    out->niter_mean = nodes ? double(s.niter_sum) / double(nodes) : 0.0;
     out->nonconverged = (int64_t)s.nonconv;
     return POND_OK;
   }

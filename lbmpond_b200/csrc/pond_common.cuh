@@ -180,6 +180,9 @@ template <typename R> struct StepArgs {
   const R* h_in = nullptr;  // [Q][N]
   R* h_out = nullptr;
   double dof = 0;           // extra degrees of freedom
+  // one-dimensional mesh schemes: node mask (nonzero = active) and node positions, or null
+  const uint8_t* mask = nullptr;  // [N]
+  const double* pos = nullptr;    // [N]
 };
 
 }  // namespace pond

@@ -43,6 +43,19 @@ struct pond_ctx {
               ev_out_free[2] = {nullptr, nullptr};
   long long pipe_k = 0;
   bool pipe_pending = false;
+  // one-dimensional mesh schemes (POND_GAP2, POND_NONUNIFORM3)
+  uint8_t* mask[2] = {nullptr, nullptr};  // node mask and the scratch copy AMR writes into
+  int mask_cur = 0;
+  long long n_active = 0;                 // active nodes in mask[mask_cur]
+  double* pos = nullptr;                  // node positions (POND_NONUNIFORM3)
+  uint8_t* amr_code = nullptr;            // coarsening: per-node transition codes [N]
+  uint32_t* amr_maps = nullptr;           // coarsening: per-chunk composed transitions
+  uint8_t* amr_sigma = nullptr;           // coarsening: automaton state entering each chunk
+  unsigned long long* amr_counts = nullptr;  // [4] device counters
+  unsigned long long* amr_counts_h = nullptr;  // pinned copy
+  // time-step adaptation after every step (update.cu:116-119)
+  bool dt_adapt = false;
+  int adapt_hi = 1000, adapt_lo = 4;
 };
 
 namespace pond {
@@ -67,4 +80,10 @@ void pipe_free(pond_ctx* c);
 int state_sums(pond_ctx* c, pond_diag* out);
 // learned path: run the bound predictor on the current state into c->guess
 int run_predictor(pond_ctx* c);
+bool mesh_scheme(int interp);
+// allocate and initialise the mask (all active) and positions (p_x = x) of a mesh context
+int mesh_alloc(pond_ctx* c);
+void mesh_free(pond_ctx* c);
+// the adaptation policy after one step: rescale the new state when NiterMax crosses a threshold
+int dt_adapt_after_step(pond_ctx* c);
 }  // namespace pond

@@ -8,6 +8,7 @@
 #include "pond_internal.h"
 #include "pond_step_1d.cuh"
 #include "pond_step_1d_energy.cuh"
+#include "pond_step_1d_mesh.cuh"
 #include "pond_step_d3q27_energy.cuh"
 #include "pond_step_d3q125_tile.cuh"
 #include "pond_step_d3q27.cuh"
@@ -36,12 +37,13 @@ int ctx_alloc(pond_ctx* c) {
   }
   if ((e = cudaMallocHost(&c->h_sums, sizeof(StepSums))) != cudaSuccess) return cuda_fail(e, "cudaMallocHost");
   std::memset(c->h_sums, 0, sizeof(StepSums));
-  return POND_OK;
+  return mesh_alloc(c);
 }
 
 void ctx_free(pond_ctx* c) {
   pipe_free(c);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  mesh_free(c);
   for (int b = 0; b < 2; b++) {
     cudaFree(c->f[b]); cudaFree(c->rho[b]); cudaFree(c->g[b]); cudaFree(c->h[b]);
     c->f[b] = c->rho[b] = c->g[b] = c->h[b] = nullptr;
@@ -113,15 +115,26 @@ int download(pond_ctx* c, const void* src, size_t count, double* dst) {
 }
 
 // ---------------------------------------------------------------- sums of a state
+// calcTotMoments (update.cu:52-69): active nodes only when a mask is given,
+// weighted by half the distance between the node's neighbours (1D, periodic)
+// when positions are given
 template <typename R>
-__global__ void state_sums_kernel(const R* rho, const R* g, long long N, double dim, double kdx, StepSums* out) {
+__global__ void state_sums_kernel(const R* rho, const R* g, long long N, double dim, double kdx, StepSums* out,
+                                  const uint8_t* mask, const double* pos) {
   const long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   NodeSums ns = {0, 0, 0, 0, 0, 0, 0ull, 0ull, 0ull, 0};
-  if (n < N) {
+  if (n < N && (mask == nullptr || mask[n] != 0)) {
     const double r = rho[n], u0 = g[n], u1 = g[N + n], u2 = g[2 * N + n], T = g[3 * N + n];
     const double u2s = u0 * u0 + u1 * u1 + u2 * u2;
-    ns.mass = r; ns.m0 = r * u0; ns.m1 = r * u1; ns.m2 = r * u2;
-    ns.enrg = r * (u2s + dim * T);
+    double d = 1.0;
+    if (pos) {
+      const double pm = pos[n == 0 ? N - 1 : n - 1];
+      double pp = pos[n + 1 == N ? 0 : n + 1];
+      if (pp < pm) pp += double(N);
+      d = 0.5 * (pp - pm);
+    }
+    ns.mass = r * d; ns.m0 = r * u0 * d; ns.m1 = r * u1 * d; ns.m2 = r * u2 * d;
+    ns.enrg = r * (u2s + dim * T) * d;
     ns.k = kdx * u2s;
   }
   reduce_and_commit(ns, out);
@@ -138,12 +151,13 @@ int state_sums(pond_ctx* c, pond_diag* out) {
   const int th = 256;
   const unsigned blocks = (unsigned)((c->N + th - 1) / th);
   const double dim = lattice_dim(c->p.lattice) + (c->p.ddf ? c->p.ddf_dof : 0);  // total energy's degrees
+  const uint8_t* mask = c->mask[0] ? c->mask[c->mask_cur] : nullptr;
   if (c->elem == 8)
     state_sums_kernel<double><<<blocks, th, 0, c->stream>>>((const double*)c->rho[c->cur], (const double*)c->g[c->cur],
-                                                            c->N, dim, kdx_of(c), c->d_sums);
+                                                            c->N, dim, kdx_of(c), c->d_sums, mask, c->pos);
   else
     state_sums_kernel<float><<<blocks, th, 0, c->stream>>>((const float*)c->rho[c->cur], (const float*)c->g[c->cur],
-                                                           c->N, dim, kdx_of(c), c->d_sums);
+                                                           c->N, dim, kdx_of(c), c->d_sums, mask, c->pos);
   StepSums s;
   e = cudaMemcpyAsync(&s, c->d_sums, sizeof(s), cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
@@ -188,6 +202,8 @@ template <typename R> static int launch_typed(pond_ctx* c, const void* const* in
   a.tol_abs = c->p.tol_abs; a.tol_rel = c->p.tol_rel;
   a.max_iter = c->p.max_iter;
   a.kdx = kdx_of(c);
+  a.mask = c->mask[0] ? c->mask[c->mask_cur] : nullptr;
+  a.pos = c->pos;
   cudaError_t e = cudaMemsetAsync(c->d_sums, 0, sizeof(StepSums), c->stream);
   if (e != cudaSuccess) return cuda_fail(e, "memset sums");
   cudaStream_t s = c->stream;
@@ -247,6 +263,12 @@ template <typename R> static int launch_typed(pond_ctx* c, const void* const* in
           break;
         case POND_WENO5:
           pull_1d_scheme_kernel<POND_WENO5, R><<<(a.nx + 127) / 128, 128, 0, s>>>(a);
+          break;
+        case POND_GAP2:
+          pull_1d_mesh_kernel<POND_GAP2, R><<<(a.nx + 127) / 128, 128, 0, s>>>(a);
+          break;
+        case POND_NONUNIFORM3:
+          pull_1d_mesh_kernel<POND_NONUNIFORM3, R><<<(a.nx + 127) / 128, 128, 0, s>>>(a);
           break;
         default: return set_error(POND_ERR_UNSUPPORTED, "scheme");
       }

@@ -22,7 +22,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liborc.so")
 
 D1Q5, D3Q27, D3Q125 = 0, 1, 2
-LAGR2, LAGR3, LAGR4, LAGR5, FIXED3, TVD, WENO5 = 2, 3, 4, 5, 6, 7, 8
+LAGR2, LAGR3, LAGR4, LAGR5, FIXED3, TVD, WENO5, GAP2, NONUNIFORM3 = 2, 3, 4, 5, 6, 7, 8, 9, 10
 BC_PERIODIC, BC_CLAMP, BC_MIRROR = 0, 1, 2
 
 # reference defaults: steps.cu:451 propagate<4> for D1Q5/D3Q27, and the
@@ -81,6 +81,14 @@ def lib():
         L.orc_set_energy.argtypes = [ctypes.c_int, ctypes.c_double, dp, ctypes.c_double, dp]
         L.orc_step_ddf.argtypes = [ctypes.POINTER(_Params), dp, dp, dp, dp, dp, dp, dp, dp, dp, ip]
         L.orc_step_ddf.restype = ctypes.c_int64
+        u8p = ctypes.POINTER(ctypes.c_uint8)
+        L.orc_step_mesh.argtypes = [ctypes.POINTER(_Params), dp, dp, dp, u8p, dp, dp, dp, dp, ip]
+        L.orc_step_mesh.restype = ctypes.c_int64
+        L.orc_amr_refine.argtypes = [ctypes.POINTER(_Params), dp, dp, dp, u8p, ctypes.c_double,
+                                     ctypes.POINTER(ctypes.c_int64)]
+        L.orc_amr_refine.restype = ctypes.c_int64
+        L.orc_amr_coarsen.argtypes = [ctypes.POINTER(_Params), dp, dp, u8p, ctypes.c_double]
+        L.orc_amr_coarsen.restype = ctypes.c_int64
         L.orc_max_threads.restype = ctypes.c_int
         _lib = L
     return _lib
@@ -228,6 +236,91 @@ def step(state: State, lattice: int, shape, interp=None, tau=0.9, tol_abs=1e-12,
     if nc < 0:
         raise ValueError("oracle step rejected its parameters")
     return out, niter, int(nc)
+
+
+def _u8p(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
+
+
+def _mesh_params(nx, interp=LAGR2, tau=0.9, tol_abs=1e-12, tol_rel=1e-10, max_iter=100, nthreads=0):
+    return _Params(D1Q5, interp, nx, 1, 1, (ctypes.c_int * 3)(BC_PERIODIC, BC_PERIODIC, BC_PERIODIC), tau,
+                   tol_abs, tol_rel, max_iter, nthreads, 0.0)
+
+
+def step_mesh(state: State, nx: int, interp=GAP2, mask=None, pos=None, tau=0.9, tol_abs=1e-12, tol_rel=1e-10,
+              max_iter=100, nthreads=0):
+    """One D1Q5 pull step on a periodic 1D mesh with a node mask (Cinfo::set;
+    None = all active) and node positions (Cell::p.x; None = p_x = x).
+    Inactive nodes are carried over unchanged.  Returns (state, niter, nonconverged)."""
+    L = lib()
+    N = nx
+    p = _mesh_params(nx, interp, tau, tol_abs, tol_rel, max_iter, nthreads)
+    f_in = np.ascontiguousarray(state.f, dtype=np.float64)
+    r_in = np.ascontiguousarray(state.rho, dtype=np.float64)
+    g_in = np.ascontiguousarray(state.g, dtype=np.float64)
+    assert f_in.shape == (5, N) and r_in.shape == (N,) and g_in.shape == (4, N)
+    mp = pp = None
+    if mask is not None:
+        mask = np.ascontiguousarray(mask, dtype=np.uint8)
+        assert mask.shape == (N,)
+        mp = _u8p(mask)
+    if pos is not None:
+        pos = np.ascontiguousarray(pos, dtype=np.float64)
+        assert pos.shape == (N,)
+        pp = _dp(pos)
+    out = State(np.empty((5, N)), np.empty(N), np.empty((4, N)))
+    niter = np.zeros(N, dtype=np.int32)
+    nc = L.orc_step_mesh(ctypes.byref(p), _dp(f_in), _dp(r_in), _dp(g_in), mp, pp,
+                         _dp(out.f), _dp(out.rho), _dp(out.g), _ip(niter))
+    if nc < 0:
+        raise ValueError("oracle mesh step rejected its parameters")
+    return out, niter, int(nc)
+
+
+def amr_refine(state: State, mask, tol=0.01):
+    """AMR_add (amr.cu:1-27) on a D1Q5 1D state; returns (state, mask, added, limit_hits)."""
+    st = state.copy()
+    m = np.array(mask, dtype=np.uint8, copy=True)
+    nx = m.size
+    p = _mesh_params(nx)
+    lim = ctypes.c_int64(0)
+    st.f = np.ascontiguousarray(st.f); st.rho = np.ascontiguousarray(st.rho); st.g = np.ascontiguousarray(st.g)
+    added = lib().orc_amr_refine(ctypes.byref(p), _dp(st.f), _dp(st.rho), _dp(st.g), _u8p(m), float(tol),
+                                 ctypes.byref(lim))
+    if added < 0:
+        raise ValueError("oracle refine rejected its parameters")
+    return st, m, int(added), int(lim.value)
+
+
+def amr_coarsen(state: State, mask, tol=0.01):
+    """AMR_remove (amr.cu:28-56); returns (mask, removed)."""
+    m = np.array(mask, dtype=np.uint8, copy=True)
+    p = _mesh_params(m.size)
+    rho = np.ascontiguousarray(state.rho, dtype=np.float64)
+    g = np.ascontiguousarray(state.g, dtype=np.float64)
+    removed = lib().orc_amr_coarsen(ctypes.byref(p), _dp(rho), _dp(g), _u8p(m), float(tol))
+    if removed < 0:
+        raise ValueError("oracle coarsen rejected its parameters")
+    return m, int(removed)
+
+
+def mesh_sums(state: State, mask=None, pos=None):
+    """calcTotMoments (update.cu:52-69) on a D1Q5 1D mesh: active nodes only,
+    each weighted by half the distance between its neighbours' positions
+    (lifted by Nx across the periodic seam) under NRMESH, else by 1."""
+    rho = state.rho
+    ux, uy, uz, T = state.g
+    nx = rho.size
+    act = np.ones(nx, dtype=bool) if mask is None else np.asarray(mask) != 0
+    if pos is None:
+        d = np.ones(nx)
+    else:
+        pm, pp = np.roll(pos, 1), np.roll(pos, -1)
+        pp = np.where(pp < pm, pp + nx, pp)
+        d = 0.5 * (pp - pm)
+    w = np.where(act, d, 0.0)
+    return {"mass": float(np.sum(rho * w)), "moment": float(np.sum(rho * ux * w)),
+            "enrg": float(np.sum(rho * (ux * ux + uy * uy + uz * uz + 1.0 * T) * w))}
 
 
 def diagnostics(state: State, lattice: int, shape):

@@ -327,6 +327,8 @@ struct Domain {
   int64_t n[3];
   int64_t N;
   int bc[3];
+  const uint8_t* mask = nullptr;  // Cinfo::set per node (nullptr: every node active)
+  const double* pos = nullptr;    // Cell::p.x per node under NRMESH (nullptr: p_x = x)
 };
 
 inline int64_t wrapi(int64_t p, int64_t n) { return ((p % n) + n) % n; }
@@ -449,6 +451,61 @@ double propagate_weno5(const Domain& D, const double crd[3], int i, const double
   return w0 * S0 + w1 * S1 + w2 * S2;
 }
 
+inline bool node_active(const Domain& D, int64_t idx) { return D.mask == nullptr || D.mask[idx] != 0; }
+inline double node_pos(const Domain& D, int64_t idx) { return D.pos ? D.pos[idx] : (double)idx; }
+
+// steps.cu:1122-1149 propagate_nonequal_1D<2>: linear interpolation at crd.x
+// between the nearest active nodes left and right of it, each found by
+// walking over inactive nodes (periodic), the shifts growing by one per node
+// passed.  1D grids (y = z = 0).
+double propagate_gap2(const Domain& D, const double crd[3], int i, const double* base, bool energy = false) {
+  const int64_t n = D.n[0];
+  const double fl = std::floor(crd[0]);
+  int64_t posL = wrapi((int64_t)fl, n), posR = wrapi((int64_t)fl + 1, n);
+  double shiftL = crd[0] - fl, shiftR = (fl + 1) - crd[0];
+  // the walks end at the latest on the (active) node being updated
+  for (int64_t k = 0; k < n && !node_active(D, posL); k++) { posL = wrapi(posL - 1, n); shiftL++; }
+  for (int64_t k = 0; k < n && !node_active(D, posR); k++) { posR = wrapi(posR + 1, n); shiftR++; }
+  Cell cl, cr;
+  load_cell(D, posL, 0, 0, cl);
+  load_cell(D, posR, 0, 0, cr);
+  return shiftR / (shiftL + shiftR) * transfer_gauge(*D.L, cl, base, i, energy) +
+         shiftL / (shiftL + shiftR) * transfer_gauge(*D.L, cr, base, i, energy);
+}
+
+// steps.cu:590-594 LagrPolNR_1D<N>: Lagrange basis on the abscissae bp[]
+double lagr_pol_nr(int N, int ix, double sx, const double* bp) {
+  double a = 1;
+  for (int ixp = 0; ixp < N; ixp++)
+    if (ixp != ix) a *= (sx - bp[ixp]) / (bp[ix] - bp[ixp]);
+  return a;
+}
+
+// steps.cu:882-908 propagateNR_1D: quadratic Lagrange interpolation at the
+// position crd_x on the node positions of x-1, x, x+1 (periodic), abscissae
+// relative to the first; a relative coordinate below -Nx/2 (integer
+// division) is lifted by Nx.
+double propagate_nonuniform3(const Domain& D, int64_t x, double crd_x, int i, const double* base,
+                             bool energy = false) {
+  const int64_t n = D.n[0];
+  const double lift = (double)((-n) / 2);
+  const int N = 3;
+  Cell c[N];
+  double bp[N];
+  const int64_t first = wrapi(x - 1, n);
+  for (int ix = 0; ix < N; ix++) {
+    const int64_t pos = wrapi(x - 1 + ix, n);
+    load_cell(D, pos, 0, 0, c[ix]);
+    bp[ix] = node_pos(D, pos) - node_pos(D, first);
+    if (bp[ix] < lift) bp[ix] += n;
+  }
+  double shift = crd_x - node_pos(D, first);
+  if (shift < lift) shift += n;
+  double fpr = 0;
+  for (int ix = 0; ix < N; ix++) fpr += lagr_pol_nr(N, ix, shift, bp) * transfer_gauge(*D.L, c[ix], base, i, energy);
+  return fpr;
+}
+
 // steps.cu:113-117 minmod
 double minmod(double a, double b) {
   if (a * b <= 0) return 0;
@@ -493,6 +550,13 @@ int pull_node(const Domain& D, const orc_params& P, int64_t x, int64_t y, int64_
   const int64_t idx = x + D.n[0] * (y + D.n[1] * z);
   Cell c0, cnew;
   load_cell(D, x, y, z, c0);
+  if (!node_active(D, idx)) {  // steps.cu:359: the step skips it; here it is carried over unchanged
+    for (int i = 0; i < L.Q; i++) f_out[(int64_t)i * D.N + idx] = c0.f[i];
+    rho_out[idx] = c0.rho;
+    for (int k = 0; k < 4; k++) g_out[(int64_t)k * D.N + idx] = c0.uT[k];
+    if (niter_out) niter_out[idx] = 0;
+    return 0;
+  }
   if (c0.rho == 0 && c0.uT[0] == 0 && c0.uT[1] == 0 && c0.uT[2] == 0 && c0.uT[3] == 0) {
     const double b[4] = {0, 0, 0, L.TLat};
     set_base(L, c0, 1, b);
@@ -541,6 +605,12 @@ int pull_node(const Domain& D, const orc_params& P, int64_t x, int64_t y, int64_
         case ORC_WENO5:
           val = propagate_weno5(D, crd, i, uT);
           if (ddf) cnew.h[i] = propagate_weno5(D, crd, i, uT, true);
+          break;
+        case ORC_GAP2:  // call site steps.cu:449
+          val = propagate_gap2(D, crd, i, uT);
+          break;
+        case ORC_NONUNIFORM3:  // call site steps.cu:453: departure point c0_st.p - v_i
+          val = propagate_nonuniform3(D, x, node_pos(D, idx) - vi[i][0], i, uT);
           break;
         default:
           val = propagate(D, P.interp, crd, i, uT);
@@ -678,6 +748,87 @@ int64_t orc_step_ddf(const orc_params* p, const double* f_in, const double* h_in
     nonconv += pull_node(D, P, x, y, z, guess, f_out, h_out, rho_out, g_out, niter);
   }
   return nonconv;
+}
+
+int64_t orc_step_mesh(const orc_params* p, const double* f_in, const double* rho_in, const double* g_in,
+                      const uint8_t* mask, const double* pos, double* f_out, double* rho_out, double* g_out,
+                      int* niter) {
+  const Lattice& L = lattice(p->lattice);
+  if (L.Q == 0 || p->nx <= 0 || p->ny <= 0 || p->nz <= 0 || p->max_iter <= 0) return -1;
+  const bool mesh_scheme = p->interp == ORC_GAP2 || p->interp == ORC_NONUNIFORM3;
+  if (mesh_scheme && (p->lattice != ORC_D1Q5 || p->ny != 1 || p->nz != 1 || p->bc[0] != ORC_BC_PERIODIC)) return -1;
+  Domain D;
+  D.L = &L;
+  D.f = f_in; D.h = nullptr; D.rho = rho_in; D.g = g_in;
+  D.n[0] = p->nx; D.n[1] = p->ny; D.n[2] = p->nz;
+  D.N = p->nx * p->ny * p->nz;
+  for (int a = 0; a < 3; a++) D.bc[a] = p->bc[a];
+  D.mask = mask;
+  D.pos = pos;
+  const orc_params P = *p;
+  int64_t nonconv = 0;
+  const int64_t N = D.N;
+#ifdef _OPENMP
+  const int nth = p->nthreads > 0 ? p->nthreads : omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : nonconv) num_threads(nth)
+#endif
+  for (int64_t n = 0; n < N; n++) {
+    const int64_t x = n % p->nx, y = (n / p->nx) % p->ny, z = n / (p->nx * p->ny);
+    nonconv += pull_node(D, P, x, y, z, nullptr, f_out, nullptr, rho_out, g_out, niter);
+  }
+  return nonconv;
+}
+
+int64_t orc_amr_refine(const orc_params* p, double* f, double* rho, double* g, uint8_t* mask, double tol,
+                       int64_t* limit_hits) {
+  const Lattice& L = lattice(p->lattice);
+  if (L.Q == 0 || p->ny != 1 || p->nz != 1 || p->nx <= 0 || !mask) return -1;
+  const int64_t nx = p->nx, N = nx;
+  const std::vector<uint8_t> set(mask, mask + nx);  // cinfo_setnew_reset: decisions read the old mask
+  int64_t added = 0, limits = 0;
+  for (int64_t x = 0; x < nx; x++) {
+    if (!set[x]) continue;
+    int64_t xp = x, dist = 0;
+    do {  // amr.cu:8-12
+      xp = (xp + 1) % nx;
+      dist++;
+    } while (!set[xp]);
+    const double vdif = g[xp] - g[x];
+    const int64_t mid = (x + dist / 2) % nx;
+    if (vdif * vdif / std::fmin(g[3 * N + x], g[3 * N + xp]) > tol || std::fabs(1 - rho[x] / rho[xp]) > tol) {
+      if (dist <= 1) limits++;
+      if (dist % 2 == 0) {  // amr.cu:18-25: the record average, saved to both time levels
+        rho[mid] = 0.5 * (rho[x] + rho[xp]);
+        for (int k = 0; k < 4; k++) g[k * N + mid] = 0.5 * (g[k * N + x] + g[k * N + xp]);
+        for (int i = 0; i < L.Q; i++) f[i * N + mid] = 0.5 * (f[i * N + x] + f[i * N + xp]);
+        if (!mask[mid]) added++;
+        mask[mid] = 1;
+      }
+    }
+  }
+  if (limit_hits) *limit_hits = limits;
+  return added;
+}
+
+int64_t orc_amr_coarsen(const orc_params* p, const double* rho, const double* g, uint8_t* mask, double tol) {
+  if (p->ny != 1 || p->nz != 1 || p->nx <= 0 || !mask) return -1;
+  const int64_t nx = p->nx, N = nx;
+  int64_t removed = 0;
+  for (int64_t ix = 0; ix < nx; ix++) {  // amr.cu:29-55, in node order, on the mask as it changes
+    if (!mask[ix]) continue;
+    int64_t xm = ix, xp = ix, distM = 0, distP = 0;
+    do { xm = (xm - 1 + nx) % nx; distM++; } while (!mask[xm]);
+    do { xp = (xp + 1) % nx; distP++; } while (!mask[xp]);
+    const double T0 = g[3 * N + ix];
+    const double vdifm = g[xm] - g[ix];
+    const double vdifp = g[xp] - g[ix];
+    if (vdifm * vdifm / T0 < tol && vdifp * vdifp / T0 < tol && std::fabs(rho[xp] / rho[ix] - 1) < tol &&
+        std::fabs(rho[xm] / rho[ix] - 1) < tol && (distM < 4 && distP < 4)) {
+      mask[ix] = 0;
+      removed++;
+    }
+  }
+  return removed;
 }
 
 int orc_max_threads(void) {

@@ -25,7 +25,9 @@ enum { ORC_D1Q5 = 0, ORC_D3Q27 = 1, ORC_D3Q125 = 2 };
 enum { ORC_LAGR2 = 2, ORC_LAGR3 = 3, ORC_LAGR4 = 4, ORC_LAGR5 = 5,
        ORC_FIXED3 = 6,   /* quadratic, stencil origin fixed at coord-1 (steps.cu:151 PonDstepD3Q125) */
        ORC_TVD = 7,      /* flux-difference minmod form (steps.cu:118 FluxTVDdif, call site :447) */
-       ORC_WENO5 = 8 };  /* propagateWENO<3,5> (steps.cu:774) */
+       ORC_WENO5 = 8,    /* propagateWENO<3,5> (steps.cu:774) */
+       ORC_GAP2 = 9,     /* linear between the nearest active nodes, propagate_nonequal_1D<2> (steps.cu:1122) */
+       ORC_NONUNIFORM3 = 10 }; /* quadratic on node positions, propagateNR_1D (steps.cu:882) */
 enum { ORC_BC_PERIODIC = 0, ORC_BC_CLAMP = 1, ORC_BC_MIRROR = 2 };
 
 typedef struct {
@@ -68,6 +70,28 @@ int64_t orc_step_ddf(const orc_params* p,
                      const double* f_in, const double* h_in, const double* rho_in, const double* g_in,
                      const double* guess,
                      double* f_out, double* h_out, double* rho_out, double* g_out, int* niter);
+/* One-dimensional mesh (D1Q5, nx x 1 x 1, periodic): orc_step with a node
+   mask (Cinfo::set, structs.cuh:92; NULL = every node active) and node
+   positions (Cell::p under NRMESH, structs.cuh:40-42; NULL = p_x = x).
+   An inactive node is skipped by the step (steps.cu:359) and copied through.
+   Schemes ORC_GAP2 and ORC_NONUNIFORM3 read the mask / the positions. */
+int64_t orc_step_mesh(const orc_params* p, const double* f_in, const double* rho_in, const double* g_in,
+                      const uint8_t* mask, const double* pos,
+                      double* f_out, double* rho_out, double* g_out, int* niter);
+/* AMR_add (amr.cu:1-27) with cinfo_setnew_reset / cinfo_set_new
+   (update.cu:30-39): every active node whose next active node to the right
+   (periodic) differs by (du)^2/min(T) > tol or |1 - rho/rho_next| > tol gets
+   the midpoint of an even gap activated, holding the average of the two
+   records (written to the state in place).  Decisions read the mask as it
+   was on entry.  Returns the nodes added; *limit_hits counts the nodes whose
+   neighbour is adjacent (the reference's "limit of cells division exceeded"). */
+int64_t orc_amr_refine(const orc_params* p, double* f, double* rho, double* g, uint8_t* mask, double tol,
+                       int64_t* limit_hits);
+/* AMR_remove (amr.cu:28-56): one serial pass in node order deactivating
+   every active node whose nearest active neighbours (in the mask as updated
+   so far) are both within 3 nodes and within tol of it in (du)^2/T and
+   density ratio.  Returns the nodes removed. */
+int64_t orc_amr_coarsen(const orc_params* p, const double* rho, const double* g, uint8_t* mask, double tol);
 int    orc_max_threads(void);
 
 #ifdef __cplusplus
