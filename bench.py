@@ -599,6 +599,54 @@ def run_configs(steps=5, warmup=2, d3q125_size=48):
     return out
 
 
+def run_mesh1d(steps=20, warmup=3, n=1 << 24):
+    """The one-dimensional mesh path on a Sod tube of n nodes (float32, tau
+    0.55, periodic): GAP2 on an AMR mask (every other node active, then one
+    refinement around the jumps) and NONUNIFORM3 on stretched positions.  Step
+    time by CUDA events on the library's stream; the state (n x 7 floats x 2
+    levels, 0.94 GB at 2^24) is far larger than L2.  Algorithmic bytes per
+    active node and step: (5 + 2) x 4 x 2 = 56 (populations, rho, u_x, T read
+    once and written once).  The AMR calls are timed by the host clock around
+    the synchronous call (which includes reading back its counts)."""
+    import lbmpond_b200 as pond
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    out = {"workload": f"D1Q5 Sod tube, {n} nodes, float32, tau 0.55, periodic", "steps": steps, "warmup": warmup}
+    sod = (0.5, 1.0, 0.0, 0.01, 0.125, 0.0, 0.008)
+    for scheme in ("GAP2", "NONUNIFORM3"):
+        with pond.Solver(lattice="D1Q5", shape=(n, 1, 1), interp=getattr(pond, scheme), precision="fp32",
+                         tau=0.55) as s:
+            s.init("sod", *sod)
+            rec = {}
+            if scheme == "GAP2":
+                s.set_mask((np.arange(n) % 2 == 0).astype(np.uint8))
+                t0 = time.perf_counter()
+                added, _ = s.amr_refine(0.01)
+                rec["refine_ms"] = (time.perf_counter() - t0) * 1e3
+                rec["refined_nodes"] = added
+            else:
+                x = np.arange(n, dtype=np.float64)
+                s.set_positions(x + 0.3 * np.sin(2 * np.pi * x / n))
+            active = int(s.get_mask().sum())
+            ms, d = _time_steps(s, steps, warmup)
+            if scheme == "GAP2":
+                t0 = time.perf_counter()
+                removed = s.amr_coarsen(0.01)
+                rec["coarsen_ms"] = (time.perf_counter() - t0) * 1e3
+                rec["coarsened_nodes"] = removed
+            gbs = 56.0 * active / (ms / 1e3) / 1e9
+            rec.update({"active_nodes": active, "ms_per_step": ms, "MLUPS": active / (ms / 1e3) / 1e6,
+                        "niter_mean": d["niter_mean"], "niter_max": d["niter_max"],
+                        "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm_peak, "unit": "GB/s",
+                                     "frac": gbs / hbm_peak, "bytes_per_node": 56}})
+            out[scheme.lower()] = rec
+    return out
+
+
 def run_reference(args, rank, world):
     """The reference arm: the reference's step restated on the host (FP64
     oracle; the reference itself has no CPU implementation), all host threads,
@@ -640,9 +688,11 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched 1D measurement")
     ap.add_argument("--batch-steps", type=int, default=1000)
     ap.add_argument("--batch-problems", type=int, default=4096)
-    ap.add_argument("--workload", default="d3q27", choices=["d3q27", "batch1d", "configs"],
-                    help="batch1d: only the batched D1Q5 measurement; configs: the other workloads (one JSON object)")
+    ap.add_argument("--workload", default="d3q27", choices=["d3q27", "batch1d", "configs", "mesh1d"],
+                    help="batch1d: only the batched D1Q5 measurement; configs: the other workloads (one JSON object); "
+                         "mesh1d: the 1D mesh path (node mask, AMR, non-uniform positions)")
     ap.add_argument("--d3q125-size", type=int, default=48)
+    ap.add_argument("--mesh-size", type=int, default=1 << 24, help="nodes of the mesh1d workload")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -664,6 +714,10 @@ def main():
             pg.destroy_process_group()
         if rank == 0:
             print(json.dumps(out), flush=True)
+        return
+    if args.workload == "mesh1d":
+        if int(os.environ.get("RANK", "0")) == 0:
+            print(json.dumps(run_mesh1d(args.steps, args.warmup, args.mesh_size)), flush=True)
         return
     if args.workload == "configs":
         if int(os.environ.get("RANK", "0")) == 0:

@@ -197,7 +197,7 @@ int pond_get_positions(pond_ctx* ctx, double* positions);
    over the threshold with an adjacent neighbour (the reference prints
    "limit of cells division exceeded").  Either output may be NULL. */
 int pond_amr_refine(pond_ctx* ctx, double tol, int64_t* added, int64_t* limit_hits);
-/* AMR_remove (amr.cu:28-56): deactivates, in one pass in node order over
+/* AMR_remove (amr.cu:28-55): deactivates, in one pass in node order over
    the mask as it changes, each active node whose nearest active neighbours
    are both within 3 nodes and within tol in (du_x)^2 / T and density ratio.
    The result equals the reference's serial pass; it is computed as a
@@ -208,7 +208,7 @@ int pond_amr_coarsen(pond_ctx* ctx, double tol, int64_t* removed);
    Multiplies every node's u by s and T by s*s in the current state (lattice
    velocities are displacements per step) and the context's dt by s; any
    lattice.  pond_set_dt_adapt applies the reference's disabled policy after
-   every step (update.cu:116-119): s = 1/2 when the step's NiterMax >= niter_hi,
+   every step (update.cu:121-123): s = 1/2 when the step's NiterMax >= niter_hi,
    s = 2 when it is <= niter_lo (the reference's values: 1000 and 4); on = 0
    turns it off.  The step's diagnostics are rescaled with the state. */
 int pond_rescale_time(pond_ctx* ctx, double s);

@@ -181,7 +181,7 @@ class Solver:
         return int(a.value), int(h.value)
 
     def amr_coarsen(self, tol=0.01):
-        """AMR_remove (amr.cu:28-56) on the current state; returns the nodes removed."""
+        """AMR_remove (amr.cu:28-55) on the current state; returns the nodes removed."""
         r = ctypes.c_int64()
         _lib.check(self._L.pond_amr_coarsen(self._ctx, float(tol), ctypes.byref(r)))
         return int(r.value)
@@ -192,7 +192,7 @@ class Solver:
         _lib.check(self._L.pond_rescale_time(self._ctx, float(s)))
 
     def set_dt_adapt(self, on=True, niter_hi=1000, niter_lo=4):
-        """After every step: dt halves when NiterMax >= niter_hi, doubles when <= niter_lo (update.cu:116-119)."""
+        """After every step: dt halves when NiterMax >= niter_hi, doubles when <= niter_lo (update.cu:121-123)."""
         _lib.check(self._L.pond_set_dt_adapt(self._ctx, 1 if on else 0, int(niter_hi), int(niter_lo)))
 
     @property

@@ -490,7 +490,7 @@ int pond_step(pond_ctx* c, int nsteps) {
     c->cur = 1 - c->cur;  // LBMParamsHost::swapLS (structs.cuh:148)
     c->istep++;
     c->curtime += c->p.dt;
-    if (c->dt_adapt) {  // update.cu:116-119, after curtime advanced by the old dt
+    if (c->dt_adapt) {  // update.cu:121-123, after curtime advanced by the old dt
       st = dt_adapt_after_step(c);
       if (st != POND_OK) return st;
     }
@@ -595,6 +595,7 @@ int pond_copy_state(pond_ctx* dst, pond_ctx* src) {
     if (e == cudaSuccess) e = cudaStreamSynchronize(dst->stream);
     if (e != cudaSuccess) return cuda_fail(e, "pond_copy_state");
     dst->n_active = src->n_active;
+    dst->part_dirty = true;
   }
   dst->initialized = true;
   dst->have_sums = false;

@@ -183,6 +183,10 @@ template <typename R> struct StepArgs {
   // one-dimensional mesh schemes: node mask (nonzero = active) and node positions, or null
   const uint8_t* mask = nullptr;  // [N]
   const double* pos = nullptr;    // [N]
+  // the nodes partitioned into the active ones and then the inactive ones,
+  // each in node order (thread t of the mesh kernels takes node part[t]), or null
+  const int* part = nullptr;      // [N]
+  long long n_active = 0;
 };
 
 }  // namespace pond

@@ -204,6 +204,12 @@ template <typename R> static int launch_typed(pond_ctx* c, const void* const* in
   a.kdx = kdx_of(c);
   a.mask = c->mask[0] ? c->mask[c->mask_cur] : nullptr;
   a.pos = c->pos;
+  if (c->mask[0]) {
+    const int pst = mesh_partition(c);
+    if (pst != POND_OK) return pst;
+    a.part = c->part;
+    a.n_active = c->n_active;
+  }
   cudaError_t e = cudaMemsetAsync(c->d_sums, 0, sizeof(StepSums), c->stream);
   if (e != cudaSuccess) return cuda_fail(e, "memset sums");
   cudaStream_t s = c->stream;

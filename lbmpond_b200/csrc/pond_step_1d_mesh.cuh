@@ -13,10 +13,13 @@
 //
 // An inactive node is skipped by the reference's step (steps.cu:359) and left
 // unwritten; here it is carried over unchanged so that the output buffer is
-// always a complete state.  The gauge iteration, moments, convergence test
-// and BGK are those of the other kernels (moments_and_test / finish_node);
-// the conservation sums cover active nodes, weighted under NONUNIFORM3 by
-// half the distance between the node's neighbours (update.cu:52-69).
+// always a complete state.  Threads take their nodes from a partition of the
+// grid (the active nodes, then the inactive ones, each in node order), so a
+// warp either steps 32 active nodes or copies 32 inactive ones whatever the
+// mask's pattern.  The gauge iteration, moments, convergence test and BGK are
+// those of the other kernels (moments_and_test / finish_node); the
+// conservation sums cover active nodes, weighted under NONUNIFORM3 by half
+// the distance between the node's neighbours (update.cu:52-69).
 #pragma once
 #include "pond_step_point.cuh"
 
@@ -46,20 +49,41 @@ __device__ __forceinline__ R transfer_one_1d(const StepArgs<R>& a, int n, int k,
 
 __device__ __forceinline__ bool mesh_active(const uint8_t* mask, int n) { return mask == nullptr || mask[n] != 0; }
 
+// periodic index of an integer-valued coordinate (a 64-bit remainder only
+// for coordinates outside [-n, 2n), which no finite gauge of the step reaches
+// in practice)
+__device__ __forceinline__ int wrap_node(double fl, int n) {
+  if (fl >= 0.0 && fl < double(n)) return int(fl);
+  if (fl >= -double(n) && fl < 0.0) return int(fl) + n;
+  if (fl >= double(n) && fl < 2.0 * double(n)) return int(fl) - n;
+  long long q = (long long)fl % n;
+  return int(q < 0 ? q + n : q);
+}
+
 template <int SCHEME, typename R>
 __global__ void __launch_bounds__(128) pull_1d_mesh_kernel(StepArgs<R> a) {
   using L = Lattice<POND_D1Q5>;
   constexpr int Q = 5;
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int x = t;
+  bool act = false;
+  if (t < a.nx) {
+    if (a.part) {
+      x = a.part[t];
+      act = t < a.n_active;
+    } else {
+      act = mesh_active(a.mask, x);
+    }
+  }
   NodeSums ns = {0, 0, 0, 0, 0, 0, 0ull, 0ull, 0ull, 0};
-  if (x < a.nx && !mesh_active(a.mask, x)) {
+  if (t < a.nx && !act) {
 #pragma unroll
     for (int q = 0; q < Q; q++) a.f_out[(long long)q * a.N + x] = a.f_in[(long long)q * a.N + x];
     a.rho_out[x] = a.rho_in[x];
 #pragma unroll
     for (int k = 0; k < 4; k++) a.g_out[(long long)k * a.N + x] = a.g_in[(long long)k * a.N + x];
     if (a.niter_out) a.niter_out[x] = 0;
-  } else if (x < a.nx) {
+  } else if (t < a.nx) {
     const int nx = a.nx;
     R f0[Q];
     double rho0, U[3], T;
@@ -68,6 +92,7 @@ __global__ void __launch_bounds__(128) pull_1d_mesh_kernel(StepArgs<R> a) {
     const int first = x == 0 ? nx - 1 : x - 1;
     int nodes[3] = {first, x, x + 1 == nx ? 0 : x + 1};
     double bp[3] = {0, 0, 0}, p_first = 0, p_x = double(x);
+    double inv[3][3];  // 1 / (bp[j] - bp[m]): the basis denominators, fixed for the step
     const double lift = double((-nx) / 2);  // -pars.Nx/2 with integer division
     if (SCHEME == POND_NONUNIFORM3) {
       p_first = a.pos ? a.pos[first] : double(first);
@@ -77,6 +102,10 @@ __global__ void __launch_bounds__(128) pull_1d_mesh_kernel(StepArgs<R> a) {
         bp[j] = (a.pos ? a.pos[nodes[j]] : double(nodes[j])) - p_first;
         if (bp[j] < lift) bp[j] += nx;
       }
+#pragma unroll
+      for (int j = 0; j < 3; j++)
+#pragma unroll
+        for (int m = 0; m < 3; m++) inv[j][m] = m == j ? 0.0 : 1.0 / (bp[j] - bp[m]);
     }
     int niter = 0;
     bool conv = false;
@@ -91,15 +120,15 @@ __global__ void __launch_bounds__(128) pull_1d_mesh_kernel(StepArgs<R> a) {
         for (int k = 0; k < Q; k++) {
           const double crd = double(x) - (C * L::xi1(k) + U[0]);
           const double fl = floor(crd);
-          long long pl = (long long)fl % nx, pr = ((long long)fl + 1) % nx;
-          if (pl < 0) pl += nx;
-          if (pr < 0) pr += nx;
+          int pl = wrap_node(fl, nx);
+          int pr = pl + 1 == nx ? 0 : pl + 1;
           double sL = crd - fl, sR = (fl + 1) - crd;
           // each walk ends at the latest on node x, which is active
-          for (int w = 0; w < nx && !mesh_active(a.mask, (int)pl); w++) { pl = pl == 0 ? nx - 1 : pl - 1; sL += 1; }
-          for (int w = 0; w < nx && !mesh_active(a.mask, (int)pr); w++) { pr = pr + 1 == nx ? 0 : pr + 1; sR += 1; }
-          const R wl = R(sR / (sL + sR)), wr = R(sL / (sL + sR));
-          acc[k] = wl * transfer_one_1d<R>(a, (int)pl, k, Uc, invC) + wr * transfer_one_1d<R>(a, (int)pr, k, Uc, invC);
+          for (int w = 0; w < nx && !mesh_active(a.mask, pl); w++) { pl = pl == 0 ? nx - 1 : pl - 1; sL += 1; }
+          for (int w = 0; w < nx && !mesh_active(a.mask, pr); w++) { pr = pr + 1 == nx ? 0 : pr + 1; sR += 1; }
+          const double isum = 1.0 / (sL + sR);
+          const R wl = R(sR * isum), wr = R(sL * isum);
+          acc[k] = wl * transfer_one_1d<R>(a, pl, k, Uc, invC) + wr * transfer_one_1d<R>(a, pr, k, Uc, invC);
         }
         ns.work += 2 * Q;
       } else {
@@ -133,7 +162,7 @@ __global__ void __launch_bounds__(128) pull_1d_mesh_kernel(StepArgs<R> a) {
             double wj = 1;
 #pragma unroll
             for (int m = 0; m < 3; m++)
-              if (m != j) wj *= (sh - bp[m]) / (bp[j] - bp[m]);
+              if (m != j) wj *= (sh - bp[m]) * inv[j][m];
             v += R(wj) * gt[j][k];
           }
           acc[k] = v;

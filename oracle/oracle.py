@@ -293,7 +293,7 @@ def amr_refine(state: State, mask, tol=0.01):
 
 
 def amr_coarsen(state: State, mask, tol=0.01):
-    """AMR_remove (amr.cu:28-56); returns (mask, removed)."""
+    """AMR_remove (amr.cu:28-55); returns (mask, removed)."""
     m = np.array(mask, dtype=np.uint8, copy=True)
     p = _mesh_params(m.size)
     rho = np.ascontiguousarray(state.rho, dtype=np.float64)

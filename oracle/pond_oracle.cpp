@@ -814,7 +814,7 @@ int64_t orc_amr_coarsen(const orc_params* p, const double* rho, const double* g,
   if (p->ny != 1 || p->nz != 1 || p->nx <= 0 || !mask) return -1;
   const int64_t nx = p->nx, N = nx;
   int64_t removed = 0;
-  for (int64_t ix = 0; ix < nx; ix++) {  // amr.cu:29-55, in node order, on the mask as it changes
+  for (int64_t ix = 0; ix < nx; ix++) {  // amr.cu:29-54, in node order, on the mask as it changes
     if (!mask[ix]) continue;
     int64_t xm = ix, xp = ix, distM = 0, distP = 0;
     do { xm = (xm - 1 + nx) % nx; distM++; } while (!mask[xm]);

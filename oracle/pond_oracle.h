@@ -87,7 +87,7 @@ int64_t orc_step_mesh(const orc_params* p, const double* f_in, const double* rho
    neighbour is adjacent (the reference's "limit of cells division exceeded"). */
 int64_t orc_amr_refine(const orc_params* p, double* f, double* rho, double* g, uint8_t* mask, double tol,
                        int64_t* limit_hits);
-/* AMR_remove (amr.cu:28-56): one serial pass in node order deactivating
+/* AMR_remove (amr.cu:28-55): one serial pass in node order deactivating
    every active node whose nearest active neighbours (in the mask as updated
    so far) are both within 3 nodes and within tol of it in (du)^2/T and
    density ratio.  Returns the nodes removed. */

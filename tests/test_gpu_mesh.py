@@ -216,7 +216,7 @@ def test_rescale_time(orc, pond, precision):
 
 def test_dt_adapt_policy(orc, pond):
     """A uniform state converges in very few iterations, so NiterMax <= 4
-    doubles dt after every step (update.cu:117-118), curtime advancing by the
+    doubles dt after every step (update.cu:121-122), curtime advancing by the
     dt in force during the step."""
     nx = 32
     with pond.Solver(lattice="D1Q5", shape=(nx, 1, 1), interp=pond.LAGR4, precision="fp64", dt=0.01) as s:

@@ -1,13 +1,13 @@
 """The oracle's one-dimensional mesh paths (CPU only): the node mask with the
 gap-bridging linear interpolation (steps.cu:1122-1149 propagate_nonequal_1D<2>),
 node positions with the non-uniform quadratic (steps.cu:882-908
-propagateNR_1D), AMR refinement and coarsening (amr.cu:1-56) and the
+propagateNR_1D), AMR refinement and coarsening (amr.cu:1-55) and the
 calcTotMoments sums (update.cu:52-69).
 
 The reference ships these disabled and has no fixtures for them, so they
 are pinned here to exact answers: the equivalences with the uniform schemes,
 polynomial reproduction across gaps and on stretched meshes, the coarsening
-pattern of a uniform field worked out by hand from amr.cu:29-55, and the
+pattern of a uniform field worked out by hand from amr.cu:29-54, and the
 C restatement against a literal Python transcription of the same loops.
 """
 import numpy as np
@@ -158,7 +158,7 @@ def test_amr_refine_known_answer(orc):
 
 
 def _coarsen_literal(rho, g, mask, tol):
-    """amr.cu:29-55, transcribed loop for loop."""
+    """amr.cu:29-54, transcribed loop for loop."""
     m = mask.copy()
     nx = m.size
     for ix in range(nx):
@@ -209,7 +209,7 @@ def test_amr_coarsen_uniform_field_keeps_every_fourth_node(orc):
 
 
 def test_mesh_step_rejects_walls(orc):
-    """The mesh schemes are periodic (steps.cu:1129-1131, :889-891)."""
+    """The mesh schemes are periodic (steps.cu:1128-1130, :891-893)."""
     import ctypes
     rho, g = sod_state(16)
     st = _base(orc, rho, g)
