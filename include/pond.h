@@ -175,11 +175,12 @@ int pond_last_step_work(pond_ctx* ctx, int64_t* work);
 
 /* ---- one-dimensional mesh: node mask, AMR, node positions -------------
    A context made with POND_GAP2 or POND_NONUNIFORM3 owns a node mask (the
-   reference's Cinfo::set, structs.cuh:90-95; all nodes active after
-   pond_create, init.cu:106).  The step skips inactive nodes (steps.cu:359)
-   and carries them over unchanged; diagnostics sum active nodes only
-   (update.cu:56-69).  A POND_NONUNIFORM3 context also owns node positions
-   (Cell::p.x under NRMESH, structs.cuh:40-42; p_x = x after pond_create,
+   reference's Cinfo::set, structs.cuh:89-94; every node active after
+   pond_create and after pond_init, whose fill sets it, init.cu:106).  The
+   step skips inactive nodes (steps.cu:359) and carries them over unchanged;
+   diagnostics sum active nodes only (update.cu:56-69).  A POND_NONUNIFORM3
+   context also owns node positions (Cell::p.x under NRMESH,
+   structs.cuh:40-42; p_x = x after pond_create and pond_init,
    init.cu:100-103) and weights the diagnostics by half the distance between
    each node's neighbours (update.cu:59-62). */
 /* mask[N] bytes, nonzero = active */

@@ -329,6 +329,7 @@ int pond_init(pond_ctx* c, int ic, const double* prm, int nprm) {
   if (e != cudaSuccess) return cuda_fail(e, "fill kernel launch");
   e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_fail(e, "fill kernel");
+  { const int ms = mesh_reset(c); if (ms != POND_OK) return ms; }  // fill sets every Cinfo::set (init.cu:106)
   c->initialized = true;
   c->istep = 0;
   c->curtime = 0;

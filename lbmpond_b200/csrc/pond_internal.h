@@ -87,6 +87,8 @@ int run_predictor(pond_ctx* c);
 bool mesh_scheme(int interp);
 // allocate and initialise the mask (all active) and positions (p_x = x) of a mesh context
 int mesh_alloc(pond_ctx* c);
+// every node active, positions p_x = x (fill, init.cu:100-106)
+int mesh_reset(pond_ctx* c);
 void mesh_free(pond_ctx* c);
 // rebuild the active/inactive partition of the nodes if the mask changed
 int mesh_partition(pond_ctx* c);

@@ -371,6 +371,12 @@ int mesh_alloc(pond_ctx* c) {
     cudaGetLastError();
     return set_error(POND_ERR_NOMEM, "node mask / positions");
   }
+  return mesh_reset(c);
+}
+
+int mesh_reset(pond_ctx* c) {
+  if (!c->mask[0]) return POND_OK;
+  const size_t N = (size_t)c->N;
   mesh::init_kernel<<<(unsigned)((N + 255) / 256), 256, 0, c->stream>>>(c->mask[0], c->pos, (long long)N);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemcpyAsync(c->mask[1], c->mask[0], N, cudaMemcpyDeviceToDevice, c->stream);
@@ -409,13 +415,17 @@ void mesh_free(pond_ctx* c) {
 }
 
 static int amr_counts(pond_ctx* c) {
-  if (c->amr_counts) return POND_OK;
-  if (cudaMalloc(&c->amr_counts, 4 * sizeof(unsigned long long)) != cudaSuccess) {
+  if (c->amr_counts && c->amr_counts_h) return POND_OK;
+  if (!c->amr_counts && cudaMalloc(&c->amr_counts, 4 * sizeof(unsigned long long)) != cudaSuccess) {
     cudaGetLastError();
+    c->amr_counts = nullptr;
     return set_error(POND_ERR_NOMEM, "AMR counters");
   }
   cudaError_t e = cudaMallocHost(&c->amr_counts_h, 4 * sizeof(unsigned long long));
-  if (e != cudaSuccess) return cuda_fail(e, "cudaMallocHost");
+  if (e != cudaSuccess) {
+    c->amr_counts_h = nullptr;
+    return cuda_fail(e, "cudaMallocHost");
+  }
   return POND_OK;
 }
 
@@ -577,11 +587,15 @@ int pond_amr_coarsen(pond_ctx* c, double tol, int64_t* removed) {
   cudaSetDevice(c->p.device);
   int st = amr_counts(c);
   if (st != POND_OK) return st;
-  if (!c->amr_code) {
+  if (!c->amr_code || !c->amr_maps || !c->amr_sigma) {
     const size_t N = (size_t)c->N, nch = (N + mesh::CHUNK - 1) / mesh::CHUNK;
+    cudaFree(c->amr_code); cudaFree(c->amr_maps); cudaFree(c->amr_sigma);
+    c->amr_code = nullptr; c->amr_maps = nullptr; c->amr_sigma = nullptr;
     if (cudaMalloc(&c->amr_code, N) != cudaSuccess || cudaMalloc(&c->amr_maps, nch * sizeof(uint32_t)) != cudaSuccess ||
         cudaMalloc(&c->amr_sigma, nch) != cudaSuccess) {
       cudaGetLastError();
+      cudaFree(c->amr_code); cudaFree(c->amr_maps); cudaFree(c->amr_sigma);
+      c->amr_code = nullptr; c->amr_maps = nullptr; c->amr_sigma = nullptr;
       return set_error(POND_ERR_NOMEM, "coarsening scratch");
     }
   }

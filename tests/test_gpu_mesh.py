@@ -251,3 +251,17 @@ def test_mesh_argument_errors(pond):
             s.amr_coarsen(0.0)
         with pytest.raises(pond.PondError):
             s.set_dt_adapt(True, 4, 4)
+
+
+def test_init_reactivates_the_mesh(pond):
+    """pond_init's fill sets every node active and p_x = x (init.cu:100-106)."""
+    nx = 64
+    with _solver(pond, nx, pond.NONUNIFORM3, "fp32") as s:
+        s.init("sod")
+        s.set_mask(np.arange(nx) % 3 == 0)
+        s.set_positions(_stretched(nx))
+        s.init("uniform")
+        assert np.array_equal(s.get_mask(), np.ones(nx, np.uint8))
+        assert np.array_equal(s.get_positions(), np.arange(nx, dtype=np.float64))
+        s.step(1)
+        assert s.diagnostics()["nonconverged"] == 0
