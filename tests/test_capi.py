@@ -137,3 +137,45 @@ def test_step_host_validates_before_device(pond):
     L = _lib.load()
     assert L.pond_step_host(None, None, None, None, None, None) == -1
     assert L.pond_sync(None) == -1
+
+
+@pytest.mark.parametrize("change,status", [
+    ({"Ny": 2}, -5),                           # the mesh schemes are one-dimensional
+    ({"Nx": 2}, -5),                           # and need three nodes for the quadratic stencil
+    ({"bc0": 1}, -5),                          # and periodic (steps.cu:1128-1130, :891-893)
+    ({"ddf": 1, "ddf_dof": 4}, -5),            # no energy populations on the mesh
+    ({"learned": 1}, -5),                      # nor the learned start
+    ({"lattice_q27": True}, -5),               # D1Q5 only
+])
+@pytest.mark.parametrize("scheme", [9, 10])  # POND_GAP2, POND_NONUNIFORM3
+def test_mesh_schemes_validate_before_device(pond, scheme, change, status):
+    from lbmpond_b200 import _lib
+    L = _lib.load()
+    p = _lib.PondParams()
+    L.pond_params_default(1 if change.get("lattice_q27") else 0, ctypes.byref(p))
+    p.interp = scheme
+    for k, v in change.items():
+        if k == "bc0":
+            p.bc[0] = v
+        elif k != "lattice_q27":
+            setattr(p, k, v)
+    ctx = ctypes.c_void_p()
+    assert L.pond_create(ctypes.byref(p), ctypes.byref(ctx)) == status
+    assert not ctx.value
+    assert L.pond_last_error_string().decode()
+
+
+def test_mesh_calls_reject_null_context(pond):
+    from lbmpond_b200 import _lib
+    L = _lib.load()
+    buf = (ctypes.c_uint8 * 4)()
+    pos = (ctypes.c_double * 4)()
+    n = ctypes.c_int64()
+    assert L.pond_set_mask(None, buf) == -1
+    assert L.pond_get_mask(None, buf) == -1
+    assert L.pond_set_positions(None, pos) == -1
+    assert L.pond_get_positions(None, pos) == -1
+    assert L.pond_amr_refine(None, 0.01, ctypes.byref(n), ctypes.byref(n)) == -1
+    assert L.pond_amr_coarsen(None, 0.01, ctypes.byref(n)) == -1
+    assert L.pond_rescale_time(None, 2.0) == -1
+    assert L.pond_set_dt_adapt(None, 1, 1000, 4) == -1
