@@ -4,7 +4,18 @@
 # the FP64 oracle against the reference and time the reference kernels on
 # the GPU; nothing in the product links them.
 #
-#   oracle/build_ref.sh <D1Q5|D3Q27|D3Q125> <double|float> <nx> <ny> <nz>
+#   oracle/build_ref.sh <D1Q5|D3Q27|D3Q125> <double|float> <nx> <ny> <nz> [scheme]
+#
+# scheme selects the interpolation call of LBMpull among the reference's own
+# alternatives at steps.cu:444-463 (the live one is propagate<4>, :451):
+#   lagr4 (default)     as shipped
+#   lagr2, lagr3, lagr5 the template order of the live call changed
+#   weno5               :451 commented, :458 propagateWENO<3,5> uncommented
+#   gap2                :451 commented, :449 propagate_nonequal_1D<2> uncommented
+#   nu3                 :451 commented, :453 propagateNR_1D uncommented, and
+#                       consts.h:12 NRMESH defined (node positions in Cell::p)
+# Only comment markers and the template argument change; the binary name
+# carries the scheme unless it is lagr4.
 #
 # The reference sources stay where they are (read-only); patched copies live
 # in a temporary directory and only the binary is written, into oracle/_ref/.
@@ -20,7 +31,8 @@ set -euo pipefail
 REF=${POND_REFERENCE_DIR:-/root/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/_ref"
-LAT=${1:?lattice}; PREC=${2:?precision}; NX=${3:?nx}; NY=${4:?ny}; NZ=${5:?nz}
+LAT=${1:?lattice}; PREC=${2:?precision}; NX=${3:?nx}; NY=${4:?ny}; NZ=${5:?nz}; SCHEME=${6:-lagr4}
+case "$SCHEME" in lagr2|lagr3|lagr4|lagr5|weno5|gap2|nu3) ;; *) echo "bad scheme $SCHEME" >&2; exit 2;; esac
 case "$LAT" in D1Q5|D3Q27|D3Q125) ;; *) echo "bad lattice $LAT" >&2; exit 2;; esac
 case "$PREC" in double|float) ;; *) echo "bad precision $PREC" >&2; exit 2;; esac
 if (( NX % 4 != 0 )); then echo "nx must be a multiple of 4 (brick.x)" >&2; exit 2; fi
@@ -28,6 +40,7 @@ if [ ! -f "$REF/steps.cu" ]; then echo "reference sources not found at $REF" >&2
 NVCC=${NVCC:-nvcc}
 mkdir -p "$OUT"
 BIN="$OUT/ref_pond_${LAT}_${PREC}_${NX}x${NY}x${NZ}"
+if [ "$SCHEME" != lagr4 ]; then BIN="${BIN}_${SCHEME}"; fi
 TMP=$(mktemp -d /tmp/pond_ref.XXXXXX)
 trap 'rm -rf "$TMP"' EXIT
 cp "$REF"/*.cu "$REF"/*.cuh "$REF"/*.h "$REF"/*.hpp "$TMP"/
@@ -36,6 +49,25 @@ grep -q "^ #define ${LAT}\$" "$TMP/consts.h"
 sed -i "s/^const long int LSizeX=.*/const long int LSizeX=$((NX / 4));/; s/^const long int LSizeY=.*/const long int LSizeY=${NY};/; s/^const long int LSizeZ=.*/const long int LSizeZ=${NZ};/" "$TMP/structs.cuh"
 sed -i 's/ptrAt\.memoryType/ptrAt.type/g' "$TMP/params.h"
 if [ "$PREC" = float ]; then sed -i 's/^#define USE_DOUBLE$/#define USE_FLOAT/' "$TMP/params.h"; fi
+LIVE='^\( *newfh = propagate *\)<4>\((make_ftype3(coord)-vi\[i\], i, uT,M4);\)$'
+grep -q "$LIVE" "$TMP/steps.cu"
+case "$SCHEME" in
+  lagr2|lagr3|lagr5) sed -i "s/$LIVE/\1<${SCHEME#lagr}>\2/" "$TMP/steps.cu" ;;
+  weno5|gap2|nu3)
+    sed -i "s/$LIVE/\/\/&/" "$TMP/steps.cu"
+    case "$SCHEME" in
+      weno5) PAT='newfh = propagateWENO<3,5>(make_ftype3(coord)-vi\[i\], i, uT, vi\[i\].x, Niter);' ;;
+      gap2)  PAT='newfh = propagate_nonequal_1D<2>(make_ftype3(coord)-vi\[i\], i, uT);' ;;
+      nu3)   PAT='newfh = propagateNR_1D(c0_st.p-vi\[i\],coord, i, uT);' ;;
+    esac
+    grep -q "^// *${PAT}\$" "$TMP/steps.cu"
+    sed -i "s/^\/\/\( *${PAT}\)\$/\1/" "$TMP/steps.cu"
+    grep -q "^ *${PAT}\$" "$TMP/steps.cu"
+    if [ "$SCHEME" = nu3 ]; then
+      sed -i 's/^\/\/ *#define NRMESH$/#define NRMESH/' "$TMP/consts.h"
+      grep -q '^#define NRMESH$' "$TMP/consts.h"
+    fi ;;
+esac
 cat > "$TMP/im2D.h" <<'EOF'
 #ifndef IM2D_H
 #define IM2D_H

@@ -4,7 +4,7 @@
 // from patched copies of engrab6/lbmPonD, into oracle/_ref/.  It replaces the
 // GL application (lbm.cu) with a file-in / file-out loop:
 //
-//   ref_pond <in.state> <out.state> <nsteps> <tau>
+//   ref_pond <in.state> <out.state> <nsteps> <tau> [<in.mesh> <out.mesh> <amr>]
 //
 // It uploads the lattice tables as lbm.cu:201-250 does, calls the reference
 // init() (init.cu:109), overwrites both population buffers with the state read
@@ -18,6 +18,15 @@
 // nz, then float64 f[Q*N], rho[N], g[4*N] (u_x,u_y,u_z,T), x fastest.  The
 // output file appends int32 NiterMax of the last step, int32 nsteps and
 // float32 kernel milliseconds per step.
+//
+// Mesh mode (the 1D adaptive-mesh code the reference's calcStep leaves
+// commented, enabled by build_ref.sh's gap2 / nu3 schemes): <in.mesh> holds
+// the node mask (Cinfo::set) and, for an NRMESH build, the node positions
+// (Cell::p.x); after every step with <amr> = 1 the driver runs
+// cinfo_setnew_reset, AMR_add, cinfo_set_new and AMR_remove in calcStep's
+// order (update.cu:102-105) before the swap.  <out.mesh> receives the final
+// mask and positions.  Mesh file: uint32 magic 0x4d455348, int64 N, uint8
+// mask[N], float64 pos[N].
 #include "structs.cuh"
 #include <cstdint>
 #include <cstdlib>
@@ -44,8 +53,36 @@ const char* FuncStr[] = {"Rho"};
 void init();
 __global__ void PonDstep();
 __global__ void PonDstepD3Q125();
+__global__ void cinfo_setnew_reset();
+__global__ void cinfo_set_new();
+__global__ void AMR_add();
+__global__ void AMR_remove();
 
 static const uint32_t MAGIC = 0x504f4e44u;
+static const uint32_t MESH_MAGIC = 0x4d455348u;
+
+static bool read_mesh(const char* fn, int64_t N, std::vector<uint8_t>& mask, std::vector<double>& pos) {
+  FILE* fp = fopen(fn, "rb");
+  if (!fp) return false;
+  uint32_t magic; int64_t n;
+  bool ok = fread(&magic, 4, 1, fp) == 1 && fread(&n, 8, 1, fp) == 1 && magic == MESH_MAGIC && n == N;
+  if (ok) {
+    mask.resize(N); pos.resize(N);
+    ok = fread(mask.data(), 1, N, fp) == (size_t)N && fread(pos.data(), 8, N, fp) == (size_t)N;
+  }
+  fclose(fp);
+  return ok;
+}
+
+static bool write_mesh(const char* fn, const std::vector<uint8_t>& mask, const std::vector<double>& pos) {
+  FILE* fp = fopen(fn, "wb");
+  if (!fp) return false;
+  const int64_t n = (int64_t)mask.size();
+  fwrite(&MESH_MAGIC, 4, 1, fp); fwrite(&n, 8, 1, fp);
+  fwrite(mask.data(), 1, mask.size(), fp); fwrite(pos.data(), 8, pos.size(), fp);
+  fclose(fp);
+  return true;
+}
 
 static bool read_state(const char* fn, int64_t n[3], std::vector<double>& f, std::vector<double>& rho,
                        std::vector<double>& g) {
@@ -65,10 +102,12 @@ static bool read_state(const char* fn, int64_t n[3], std::vector<double>& f, std
 }
 
 int main(int argc, char** argv) {
-  if (argc < 5) {
-    fprintf(stderr, "usage: %s in.state out.state nsteps tau\n", argv[0]);
+  if (argc < 5 || (argc > 5 && argc != 8)) {
+    fprintf(stderr, "usage: %s in.state out.state nsteps tau [in.mesh out.mesh amr]\n", argv[0]);
     return 2;
   }
+  const bool mesh = argc == 8;
+  const bool amr = mesh && atoi(argv[7]) != 0;
   const int nsteps = atoi(argv[3]);
   const double tau = atof(argv[4]);
   int64_t n[3];
@@ -122,6 +161,20 @@ int main(int argc, char** argv) {
   CHECK_ERROR(cudaDeviceSynchronize());
 
   const int64_t N = n[0] * n[1] * n[2];
+  std::vector<uint8_t> mask(N, 1);
+  std::vector<double> pos(N);
+  for (int64_t i = 0; i < N; i++) pos[i] = double(i % n[0]);  // init.cu:102
+  if (mesh) {
+    if (!read_mesh(argv[5], N, mask, pos)) { fprintf(stderr, "bad mesh file %s\n", argv[5]); return 3; }
+    std::vector<Cinfo> ci(N);
+    for (int64_t i = 0; i < N; i++) {
+      const int x = i % n[0], y = (i / n[0]) % n[1], z = i / (n[0] * n[1]);
+      Cinfo& c = ci[Cinfo::ind_zip(x, y, z)];
+      c.ctype = 0; c.niter = 0;
+      c.set = c.setnew = mask[i] ? 1 : 0;
+    }
+    CHECK_ERROR(cudaMemcpy(parsHost.cinfo, ci.data(), N * sizeof(Cinfo), cudaMemcpyHostToDevice));
+  }
   std::vector<Group> gh(N);
   for (int64_t i = 0; i < N; i++) {
     Cell c;
@@ -129,6 +182,9 @@ int main(int argc, char** argv) {
     c.rho = (ftype)rho[i];
     c.uT = make_ftype4((ftype)g[i], (ftype)g[N + i], (ftype)g[2 * N + i], (ftype)g[3 * N + i]);
     const int x = i % n[0], y = (i / n[0]) % n[1], z = i / (n[0] * n[1]);
+#ifdef NRMESH
+    c.p = make_ftype3((ftype)pos[i], (ftype)y, (ftype)z);
+#endif
     const int2 gc = Group::ind_conv(x, y, z);
     gh[gc.x].pack(c, gc.y);
   }
@@ -146,10 +202,10 @@ int main(int argc, char** argv) {
     CHECK_ERROR(cudaMemset(parsHost.enrg, 0, sizeof(ftype)));
     CHECK_ERROR(cudaMemset(parsHost.moment, 0, sizeof(ftype3)));
     CHECK_ERROR(cudaEventRecord(t0));
+    const dim3 block(parsHost.Nx / brick.x, parsHost.Ny / brick.y, parsHost.Nz / brick.z);
 #if defined D3Q125
     PonDstepD3Q125<<<dim3(parsHost.Nx, parsHost.Ny, parsHost.Nz), Qn>>>();
 #else
-    dim3 block(parsHost.Nx / brick.x, parsHost.Ny / brick.y, parsHost.Nz / brick.z);
     PonDstep<<<block, brick>>>();
 #endif
     CHECK_ERROR(cudaEventRecord(t1));
@@ -157,6 +213,14 @@ int main(int argc, char** argv) {
     CHECK_ERROR(cudaGetLastError());
     CHECK_ERROR(cudaEventElapsedTime(&ms[s], t0, t1));
     niter_max = *parsHost.NiterMax;
+    if (amr) {  // update.cu:102-105 with the AMR lines enabled, on the store buffer before the swap
+      cinfo_setnew_reset<<<block, brick>>>();
+      AMR_add<<<block, brick>>>();
+      cinfo_set_new<<<block, brick>>>();
+      AMR_remove<<<1, 1>>>();
+      CHECK_ERROR(cudaDeviceSynchronize());
+      CHECK_ERROR(cudaGetLastError());
+    }
     parsHost.iStep++;
     parsHost.swapLS();
     copy2dev(parsHost, pars);
@@ -170,6 +234,18 @@ int main(int argc, char** argv) {
     for (int q = 0; q < Qn; q++) f[(size_t)q * N + i] = c.f[q];
     rho[i] = c.rho;
     g[i] = c.uT.x; g[N + i] = c.uT.y; g[2 * N + i] = c.uT.z; g[3 * N + i] = c.uT.w;
+#ifdef NRMESH
+    pos[i] = c.p.x;
+#endif
+  }
+  if (mesh) {
+    std::vector<Cinfo> ci(N);
+    CHECK_ERROR(cudaMemcpy(ci.data(), parsHost.cinfo, N * sizeof(Cinfo), cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < N; i++) {
+      const int x = i % n[0], y = (i / n[0]) % n[1], z = i / (n[0] * n[1]);
+      mask[i] = ci[Cinfo::ind_zip(x, y, z)].set ? 1 : 0;
+    }
+    if (!write_mesh(argv[6], mask, pos)) { fprintf(stderr, "cannot write %s\n", argv[6]); return 5; }
   }
   FILE* fp = fopen(argv[2], "wb");
   if (!fp) { fprintf(stderr, "cannot write %s\n", argv[2]); return 5; }

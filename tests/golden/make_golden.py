@@ -9,6 +9,12 @@ Each case stores the seeded input state, the number of steps, tau and the
 reference's output state (float64, host layout f[Q,N], rho[N], g[4,N]).
 The reference has no golden files or tests of its own; these fixtures are the
 pin between it and the FP64 oracle (tests/test_golden.py).
+
+Cases with a ``scheme`` run one of the reference's alternative interpolation
+calls (steps.cu:444-463, selected by oracle/build_ref.sh's scheme argument);
+cases with a ``mesh`` also pass a node mask and node positions, and with
+``amr`` the reference's AMR kernels run after every step.  ``--only`` makes a
+subset (names containing any of the given words).
 """
 from __future__ import annotations
 
@@ -56,6 +62,26 @@ def read_state(path, Q, shape):
     return f, rho, g, niter_max, ms
 
 
+MESH_MAGIC = 0x4D455348
+
+
+def write_mesh(path, mask, pos):
+    with open(path, "wb") as fp:
+        np.array([MESH_MAGIC], dtype=np.uint32).tofile(fp)
+        np.array([mask.size], dtype=np.int64).tofile(fp)
+        np.ascontiguousarray(mask, dtype=np.uint8).tofile(fp)
+        np.ascontiguousarray(pos, dtype=np.float64).tofile(fp)
+
+
+def read_mesh(path, N):
+    with open(path, "rb") as fp:
+        assert int(np.fromfile(fp, dtype=np.uint32, count=1)[0]) == MESH_MAGIC
+        assert int(np.fromfile(fp, dtype=np.int64, count=1)[0]) == N
+        mask = np.fromfile(fp, dtype=np.uint8, count=N)
+        pos = np.fromfile(fp, dtype=np.float64, count=N)
+    return mask, pos
+
+
 def acoustic(nx, T0=0.1, A=0.02, gamma=3.0):
     """init.cu:43-50 (the reference's shipped initial condition)."""
     x = np.arange(nx)
@@ -65,6 +91,43 @@ def acoustic(nx, T0=0.1, A=0.02, gamma=3.0):
     u = A * np.sin(x * 2 * np.pi / nx) * T0 / np.sqrt(gamma * T0)
     z = np.zeros(nx)
     return rho, np.stack([u, z, z, T])
+
+
+def sparse_mask(nx, seed, density=0.7):
+    """A seeded node mask with at most four inactive nodes in a row."""
+    rng = np.random.default_rng(seed)
+    m = (rng.random(nx) < density).astype(np.uint8)
+    m[::5] = 1
+    return m
+
+
+def stretched(nx, amp=0.3):
+    x = np.arange(nx, dtype=np.float64)
+    return x + amp * np.sin(2 * np.pi * x / nx)
+
+
+def scheme_cases():
+    """Alternative interpolation calls and the 1D mesh: dicts with the keys of
+    cases() plus scheme, and mesh = (mask, positions, amr) for mesh runs."""
+    out = []
+
+    def add(name, lat, shape, tau, nsteps, state, pseed, scheme, mesh=None):
+        out.append(dict(name=name, lat=lat, shape=shape, tau=tau, nsteps=nsteps, state=state, pseed=pseed,
+                        scheme=scheme, mesh=mesh))
+
+    for scheme, seed in (("lagr2", 21), ("lagr3", 22), ("lagr5", 23)):
+        add(f"d1q5_{scheme}_128", 0, (128, 1, 1), 0.7, 5, smooth_state((128, 1, 1), 1, seed=seed, modes=2), seed,
+            scheme)
+    add("d1q5_weno5_sod_128", 0, (128, 1, 1), 0.55, 6, sod_state(128, (1.0, 0.0, 0.01), (0.125, 0.0, 0.008)), None,
+        "weno5")
+    add("d3q27_lagr3_8", 1, (8, 8, 8), 0.8, 2, smooth_state((8, 8, 8), 3, seed=24, modes=1, du=0.03), 24, "lagr3")
+    add("d1q5_gap2_mask_128", 0, (128, 1, 1), 0.7, 4, smooth_state((128, 1, 1), 1, seed=25, modes=2), 25, "gap2",
+        (sparse_mask(128, 25), np.arange(128, dtype=np.float64), 0))
+    add("d1q5_gap2_amr_sod_128", 0, (128, 1, 1), 0.6, 6, sod_state(128, (1.0, 0.0, 0.01), (0.125, 0.0, 0.008)),
+        None, "gap2", ((np.arange(128) % 2 == 0).astype(np.uint8), np.arange(128, dtype=np.float64), 1))
+    add("d1q5_nu3_128", 0, (128, 1, 1), 0.7, 4, smooth_state((128, 1, 1), 1, seed=26, modes=2), 26, "nu3",
+        (np.ones(128, np.uint8), stretched(128), 0))
+    return out
 
 
 def cases():
@@ -80,28 +143,52 @@ def cases():
     return out
 
 
+def all_cases():
+    out = [dict(name=name, lat=lat, shape=shape, tau=tau, nsteps=nsteps, state=state, pseed=pseed, scheme="lagr4",
+                mesh=None) for name, lat, shape, tau, nsteps, state, pseed in cases()]
+    return out + scheme_cases()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(ROOT, "tests", "golden"))
     ap.add_argument("--refdir", default=os.path.join(ROOT, "oracle", "_ref"))
+    ap.add_argument("--only", nargs="*", default=None)
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
-    for name, lat, shape, tau, nsteps, (rho, g), pseed in cases():
+    for c in all_cases():
+        name, lat, shape, tau, nsteps, (rho, g), pseed = (c[k] for k in ("name", "lat", "shape", "tau", "nsteps",
+                                                                          "state", "pseed"))
+        if args.only and not any(w in name for w in args.only):
+            continue
         t = O.tables(lat)
         f = t.w[:, None] * rho[None, :]
         if pseed is not None:
             f = perturbed_populations(O, lat, rho, g, seed=pseed)
         binary = os.path.join(args.refdir, f"ref_pond_{LAT_NAME[lat]}_double_{shape[0]}x{shape[1]}x{shape[2]}")
+        if c["scheme"] != "lagr4":
+            binary += "_" + c["scheme"]
+        extra = {}
         with tempfile.TemporaryDirectory() as td:
             fin, fout = os.path.join(td, "in.state"), os.path.join(td, "out.state")
             write_state(fin, f, rho, g, shape)
-            r = subprocess.run([binary, fin, fout, str(nsteps), repr(tau)], capture_output=True, text=True)
+            cmd = [binary, fin, fout, str(nsteps), repr(tau)]
+            if c["mesh"] is not None:
+                mask, pos, amr = c["mesh"]
+                min_, mout = os.path.join(td, "in.mesh"), os.path.join(td, "out.mesh")
+                write_mesh(min_, mask, pos)
+                cmd += [min_, mout, str(amr)]
+            r = subprocess.run(cmd, capture_output=True, text=True)
             if r.returncode != 0:
                 raise SystemExit(f"{name}: reference run failed ({r.returncode})\n{r.stdout}\n{r.stderr}")
             fo, ro, go, niter_max, ms = read_state(fout, t.Q, shape)
+            if c["mesh"] is not None:
+                mo, po = read_mesh(mout, int(np.prod(shape)))
+                extra = dict(mask_in=mask, pos_in=pos, amr=amr, mask_out=mo, pos_out=po,
+                             limit_lines=r.stdout.count("limit of cells division exceeded"))
         np.savez_compressed(os.path.join(args.out, name + ".npz"), lattice=lat, shape=np.array(shape), tau=tau,
                             nsteps=nsteps, f_in=f, rho_in=rho, g_in=g, f_out=fo, rho_out=ro, g_out=go,
-                            niter_max=niter_max, kernel_ms=ms)
+                            niter_max=niter_max, kernel_ms=ms, scheme=c["scheme"], **extra)
         print(f"{name}: NiterMax={niter_max} kernel ms/step={ms.mean():.3f}")
 
 
