@@ -74,3 +74,39 @@ def test_oracle_matches_reference_kernels(orc, path):
     assert np.abs(st.g[3][sel] - T).max() <= 1e-9 * np.abs(T).max()
     cs = np.sqrt(np.abs(T).max())
     assert np.abs(st.g[:3][:, sel] - g_out[:3]).max() <= 1e-9 * cs
+
+
+def test_mesh_file_roundtrip(tmp_path):
+    """The mesh file of make_golden.py / oracle/ref_main.cu (magic, N, mask, positions)."""
+    from tests.golden.make_golden import read_mesh, write_mesh
+    mask = (np.arange(37) % 3 != 0).astype(np.uint8)
+    pos = np.arange(37) + 0.25
+    path = str(tmp_path / "m.mesh")
+    write_mesh(path, mask, pos)
+    m, p = read_mesh(path, 37)
+    assert np.array_equal(m, mask) and np.array_equal(p, pos)
+    raw = np.fromfile(path, dtype=np.uint32, count=1)
+    assert int(raw[0]) == 0x4D455348
+
+
+@pytest.mark.parametrize("idx", range(8))
+def test_scheme_cases_replay_cleanly(orc, idx):
+    """Every alternative-scheme and mesh case converges everywhere in the oracle,
+    so a fixture made from it by the reference's kernels compares node by node."""
+    from tests.golden.make_golden import scheme_cases
+    from tests.states import perturbed_populations
+    cases = scheme_cases()
+    assert len(cases) == 8
+    c = cases[idx]
+    rho, g = c["state"]
+    t = orc.tables(c["lat"])
+    f = t.w[:, None] * rho[None, :] if c["pseed"] is None else perturbed_populations(orc, c["lat"], rho, g,
+                                                                                      seed=c["pseed"])
+    z = dict(lattice=c["lat"], shape=np.array(c["shape"]), tau=c["tau"], nsteps=c["nsteps"], f_in=f, rho_in=rho,
+             g_in=g, scheme=c["scheme"])
+    if c["mesh"] is not None:
+        z.update(mask_in=c["mesh"][0], pos_in=c["mesh"][1], amr=c["mesh"][2])
+    st, niter, mask = replay(orc, z)
+    assert np.isfinite(st.f).all() and int(niter.max()) < 100
+    if mask is not None:
+        assert 0 < int(mask.sum()) <= mask.size
