@@ -145,6 +145,9 @@ int pond_get_fields(pond_ctx* ctx, double* rho, double* ux, double* uy, double* 
 /* advance nsteps steps (calcStep without drop/diagnostics printing) */
 int pond_step(pond_ctx* ctx, int nsteps);
 int pond_diagnostics(pond_ctx* ctx, pond_diag* out);
+/* the step counter, simulated time and dt of a resumed run (LBMParamsHost
+   iStep / curtime / dt); dt <= 0 keeps the current dt.  Host bookkeeping only. */
+int pond_set_clock(pond_ctx* ctx, int64_t istep, double curtime, double dt);
 /* per-node iteration counts of the last step (int32[N]); needs pond_keep_niter(ctx, 1) before the step */
 int pond_keep_niter(pond_ctx* ctx, int on);
 int pond_get_niter(pond_ctx* ctx, int32_t* niter);

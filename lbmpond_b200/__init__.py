@@ -197,9 +197,29 @@ class Solver:
 
     @property
     def dt(self) -> float:
+        return float(self.get_params().dt)
+
+    def get_params(self):
+        """The context's current pond_params (dt follows rescalings)."""
         p = _lib.PondParams()
         _lib.check(self._L.pond_get_params(self._ctx, ctypes.byref(p)))
-        return float(p.dt)
+        return p
+
+    def set_clock(self, istep, curtime, dt=0.0):
+        """Step counter, simulated time and (if > 0) dt of a resumed run."""
+        _lib.check(self._L.pond_set_clock(self._ctx, int(istep), float(curtime), float(dt)))
+
+    # -- checkpoint / resume (no counterpart in the reference)
+    def checkpoint(self, path):
+        """Write everything the next step reads to one .npz (lbmpond_b200.checkpoint)."""
+        from . import checkpoint
+        checkpoint.save(self, path)
+
+    @classmethod
+    def resume(cls, path, device=0) -> "Solver":
+        """A new Solver continuing a checkpointed run."""
+        from . import checkpoint
+        return checkpoint.load(path, device)
 
     def keep_niter(self, on=True):
         _lib.check(self._L.pond_keep_niter(self._ctx, 1 if on else 0))

@@ -613,6 +613,16 @@ int pond_last_step_work(pond_ctx* c, int64_t* work) {
   return POND_OK;
 }
 
+int pond_set_clock(pond_ctx* c, int64_t istep, double curtime, double dt) {
+  if (!c) return set_error(POND_ERR_ARG, "null context");
+  if (istep < 0 || !std::isfinite(curtime) || !std::isfinite(dt))
+    return set_error(POND_ERR_ARG, "pond_set_clock: istep >= 0, finite time and dt");
+  c->istep = istep;
+  c->curtime = curtime;
+  if (dt > 0) c->p.dt = dt;
+  return POND_OK;
+}
+
 int pond_diagnostics(pond_ctx* c, pond_diag* out) {
   if (!c || !out) return set_error(POND_ERR_ARG, "null argument");
   { const int ps = pipe_drain(c); if (ps != POND_OK) return ps; }
