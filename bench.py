@@ -36,6 +36,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from lbmpond_b200 import configs  # noqa: E402  (initial conditions; loads no library)
+
 METRIC = "MLUPS D3Q27 256^3: learned-gauge vs plain PonD at equal L1 error vs FP64"
 LAMBDA = 0.25            # dt/dx of the lattice
 TAU = 0.52
@@ -46,19 +48,12 @@ NOMINAL_FP32_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 148 SMs x 128 lanes x FM
 
 def sphere_params():
     # cx, cy, cz, radius, rho_in, T_in, rho_out, T_out  (T = lambda^2 p/rho)
-    return (0.5, 0.5, 0.5, 0.2, 1.0, LAMBDA ** 2 * 1.0, 0.125, LAMBDA ** 2 * 0.1 / 0.125)
+    return configs.sphere_params(LAMBDA)
 
 
 def sphere_state(n):
     """The same initial condition on the host (for the oracle's sample)."""
-    c = (np.arange(n) + 0.5) / n - 0.5
-    z, y, x = np.meshgrid(c, c, c, indexing="ij")
-    inside = (x * x + y * y + z * z < 0.2 ** 2).reshape(-1)
-    p = sphere_params()
-    rho = np.where(inside, p[4], p[6])
-    T = np.where(inside, p[5], p[7])
-    zero = np.zeros_like(rho)
-    return rho, np.stack([zero, zero, zero, T])
+    return configs.sphere_state(n, LAMBDA)
 
 
 # ------------------------------------------------------------------ clocks
@@ -451,28 +446,7 @@ def _time_steps(s, steps, warmup):
     return float(np.mean(ms)), s.diagnostics()
 
 
-def shock_vortex_state(n, mach=1.5, T1=0.1, eps=0.3, radius=0.05, gamma=5.0 / 3.0):
-    """Stationary normal shock at x = 0.5 (pre-shock rho = 1, T = T1, flow
-    along +x at `mach`; post-shock state from the Rankine-Hugoniot
-    relations) and an isentropic vortex of strength `eps` (velocity scale
-    eps * c1) and radius `radius` at (0.25, 0.5) in x, y on the unit box, in
-    lattice units of the D3Q125 gauge (TLat = 1).  gamma = 5/3 is the
-    monatomic 3D gas the step models."""
-    x = (np.arange(n) + 0.5) / n
-    X, Y, _ = np.meshgrid(x, x, x, indexing="ij")  # [x, y, z]
-    c1 = np.sqrt(gamma * T1)
-    u1 = mach * c1
-    r21 = (gamma + 1) * mach ** 2 / ((gamma - 1) * mach ** 2 + 2)
-    p21 = 1 + 2 * gamma / (gamma + 1) * (mach ** 2 - 1)
-    pre = X < 0.5
-    dx, dy = X - 0.25, Y - 0.5
-    e = np.exp(0.5 * (1 - (dx * dx + dy * dy) / radius ** 2)) * pre
-    ux = np.where(pre, u1, u1 / r21) - eps * c1 * dy / radius * e
-    uy = eps * c1 * dx / radius * e
-    T = np.where(pre, T1, T1 * p21 / r21) * (1 - (gamma - 1) / 2 * eps ** 2 * e * e)
-    rho = np.where(pre, (1 - (gamma - 1) / 2 * eps ** 2 * e * e) ** (1 / (gamma - 1)), r21)
-    flat = lambda a: np.ascontiguousarray(a.transpose(2, 1, 0)).ravel()  # x fastest
-    return flat(rho), np.stack([flat(ux), flat(uy), np.zeros(n ** 3), flat(T)])
+shock_vortex_state = configs.shock_vortex_state
 
 
 def run_configs(steps=5, warmup=2, d3q125_size=48):
