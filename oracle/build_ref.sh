@@ -4,7 +4,7 @@
 # the FP64 oracle against the reference and time the reference kernels on
 # the GPU; nothing in the product links them.
 #
-#   oracle/build_ref.sh <D1Q5|D3Q27|D3Q125> <double|float> <nx> <ny> <nz> [scheme]
+#   oracle/build_ref.sh <D1Q5|D3Q27|D3Q125> <double|float> <nx> <ny> <nz> [scheme] [bc]
 #
 # scheme selects the interpolation call of LBMpull among the reference's own
 # alternatives at steps.cu:444-463 (the live one is propagate<4>, :451):
@@ -16,6 +16,14 @@
 #                       consts.h:12 NRMESH defined (node positions in Cell::p)
 # Only comment markers and the template argument change; the binary name
 # carries the scheme unless it is lagr4.
+#
+# bc = mirror sets the `outflow` flags of steps.cu; on the D1Q5 / D3Q27 path
+# only propagate<N>'s counts (steps.cu:1004-1013): the stencil is reflected
+# at every face with the populations reversed (Cell::mirrX/Y/Z,
+# structs.cuh:552-578).  periodic (default) leaves them off.  With the
+# Lagrange schemes only (the other propagators never read the flag), and not
+# on D3Q125, whose flag (steps.cu:373) moves x positions without reversing
+# populations.
 #
 # The reference sources stay where they are (read-only); patched copies live
 # in a temporary directory and only the binary is written, into oracle/_ref/.
@@ -31,7 +39,13 @@ set -euo pipefail
 REF=${POND_REFERENCE_DIR:-/root/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/_ref"
-LAT=${1:?lattice}; PREC=${2:?precision}; NX=${3:?nx}; NY=${4:?ny}; NZ=${5:?nz}; SCHEME=${6:-lagr4}
+LAT=${1:?lattice}; PREC=${2:?precision}; NX=${3:?nx}; NY=${4:?ny}; NZ=${5:?nz}; SCHEME=${6:-lagr4}; BC=${7:-periodic}
+case "$BC" in
+  periodic) ;;
+  mirror) [ "$LAT" != D3Q125 ] || { echo "mirror: D1Q5 and D3Q27 only" >&2; exit 2; }
+          case "$SCHEME" in lagr*) ;; *) echo "mirror: Lagrange schemes only" >&2; exit 2;; esac ;;
+  *) echo "bad bc $BC" >&2; exit 2;;
+esac
 case "$SCHEME" in lagr2|lagr3|lagr4|lagr5|weno5|gap2|nu3) ;; *) echo "bad scheme $SCHEME" >&2; exit 2;; esac
 case "$LAT" in D1Q5|D3Q27|D3Q125) ;; *) echo "bad lattice $LAT" >&2; exit 2;; esac
 case "$PREC" in double|float) ;; *) echo "bad precision $PREC" >&2; exit 2;; esac
@@ -41,6 +55,7 @@ NVCC=${NVCC:-nvcc}
 mkdir -p "$OUT"
 BIN="$OUT/ref_pond_${LAT}_${PREC}_${NX}x${NY}x${NZ}"
 if [ "$SCHEME" != lagr4 ]; then BIN="${BIN}_${SCHEME}"; fi
+if [ "$BC" = mirror ]; then BIN="${BIN}_mirror"; fi
 TMP=$(mktemp -d /tmp/pond_ref.XXXXXX)
 trap 'rm -rf "$TMP"' EXIT
 cp "$REF"/*.cu "$REF"/*.cuh "$REF"/*.h "$REF"/*.hpp "$TMP"/
@@ -49,6 +64,10 @@ grep -q "^ #define ${LAT}\$" "$TMP/consts.h"
 sed -i "s/^const long int LSizeX=.*/const long int LSizeX=$((NX / 4));/; s/^const long int LSizeY=.*/const long int LSizeY=${NY};/; s/^const long int LSizeZ=.*/const long int LSizeZ=${NZ};/" "$TMP/structs.cuh"
 sed -i 's/ptrAt\.memoryType/ptrAt.type/g' "$TMP/params.h"
 if [ "$PREC" = float ]; then sed -i 's/^#define USE_DOUBLE$/#define USE_FLOAT/' "$TMP/params.h"; fi
+if [ "$BC" = mirror ]; then
+  [ "$(grep -c '^    const bool outflow=0;$' "$TMP/steps.cu")" -ge 1 ]
+  sed -i 's/^    const bool outflow=0;$/    const bool outflow=1;/' "$TMP/steps.cu"
+fi
 LIVE='^\( *newfh = propagate *\)<4>\((make_ftype3(coord)-vi\[i\], i, uT,M4);\)$'
 grep -q "$LIVE" "$TMP/steps.cu"
 case "$SCHEME" in

@@ -13,7 +13,8 @@ pin between it and the FP64 oracle (tests/test_golden.py).
 Cases with a ``scheme`` run one of the reference's alternative interpolation
 calls (steps.cu:444-463, selected by oracle/build_ref.sh's scheme argument);
 cases with a ``mesh`` also pass a node mask and node positions, and with
-``amr`` the reference's AMR kernels run after every step.  ``--only`` makes a
+``amr`` the reference's AMR kernels run after every step; cases with
+``bc = mirror`` run the reference's disabled mirror walls.  ``--only`` makes a
 subset (names containing any of the given words).
 """
 from __future__ import annotations
@@ -111,9 +112,9 @@ def scheme_cases():
     cases() plus scheme, and mesh = (mask, positions, amr) for mesh runs."""
     out = []
 
-    def add(name, lat, shape, tau, nsteps, state, pseed, scheme, mesh=None):
+    def add(name, lat, shape, tau, nsteps, state, pseed, scheme, mesh=None, bc="periodic"):
         out.append(dict(name=name, lat=lat, shape=shape, tau=tau, nsteps=nsteps, state=state, pseed=pseed,
-                        scheme=scheme, mesh=mesh))
+                        scheme=scheme, mesh=mesh, bc=bc))
 
     for scheme, seed in (("lagr2", 21), ("lagr3", 22), ("lagr5", 23)):
         add(f"d1q5_{scheme}_128", 0, (128, 1, 1), 0.7, 5, smooth_state((128, 1, 1), 1, seed=seed, modes=2), seed,
@@ -127,6 +128,11 @@ def scheme_cases():
         None, "gap2", ((np.arange(128) % 2 == 0).astype(np.uint8), np.arange(128, dtype=np.float64), 1))
     add("d1q5_nu3_128", 0, (128, 1, 1), 0.7, 4, smooth_state((128, 1, 1), 1, seed=26, modes=2), 26, "nu3",
         (np.ones(128, np.uint8), stretched(128), 0))
+    # the reference's disabled mirror walls (propagate<N>'s outflow flag, steps.cu:1004-1013)
+    add("d1q5_mirror_128", 0, (128, 1, 1), 0.7, 5, smooth_state((128, 1, 1), 1, seed=27, modes=2, du=0.03), 27,
+        "lagr4", bc="mirror")
+    add("d3q27_mirror_8", 1, (8, 8, 8), 0.8, 2, smooth_state((8, 8, 8), 3, seed=28, modes=1, du=0.03), 28, "lagr4",
+        bc="mirror")
     return out
 
 
@@ -145,7 +151,7 @@ def cases():
 
 def all_cases():
     out = [dict(name=name, lat=lat, shape=shape, tau=tau, nsteps=nsteps, state=state, pseed=pseed, scheme="lagr4",
-                mesh=None) for name, lat, shape, tau, nsteps, state, pseed in cases()]
+                mesh=None, bc="periodic") for name, lat, shape, tau, nsteps, state, pseed in cases()]
     return out + scheme_cases()
 
 
@@ -168,6 +174,8 @@ def main():
         binary = os.path.join(args.refdir, f"ref_pond_{LAT_NAME[lat]}_double_{shape[0]}x{shape[1]}x{shape[2]}")
         if c["scheme"] != "lagr4":
             binary += "_" + c["scheme"]
+        if c["bc"] == "mirror":
+            binary += "_mirror"
         extra = {}
         with tempfile.TemporaryDirectory() as td:
             fin, fout = os.path.join(td, "in.state"), os.path.join(td, "out.state")
@@ -188,7 +196,7 @@ def main():
                              limit_lines=r.stdout.count("limit of cells division exceeded"))
         np.savez_compressed(os.path.join(args.out, name + ".npz"), lattice=lat, shape=np.array(shape), tau=tau,
                             nsteps=nsteps, f_in=f, rho_in=rho, g_in=g, f_out=fo, rho_out=ro, g_out=go,
-                            niter_max=niter_max, kernel_ms=ms, scheme=c["scheme"], **extra)
+                            niter_max=niter_max, kernel_ms=ms, scheme=c["scheme"], bc=c["bc"], **extra)
         print(f"{name}: NiterMax={niter_max} kernel ms/step={ms.mean():.3f}")
 
 

@@ -171,8 +171,9 @@ def test_matches_reference_fixtures_directly(pond):
         lat = int(z["lattice"]); shape = tuple(int(v) for v in z["shape"])
         scheme = str(z["scheme"]) if "scheme" in z.files else "lagr4"
         sel = slice(None)
+        bc = ("mirror",) * 3 if "bc" in z.files and str(z["bc"]) == "mirror" else ("periodic",) * 3
         with pond.Solver(lattice=lat, shape=shape, precision="fp64", tau=float(z["tau"]),
-                         interp=SCHEME_INTERP[scheme]) as s:
+                         interp=SCHEME_INTERP[scheme], bc=bc) as s:
             s.set_state(z["rho_in"], z["g_in"], f=z["f_in"])
             if "mask_in" in z.files:  # the 1D mesh (make_golden.py scheme_cases)
                 s.set_mask(z["mask_in"])
