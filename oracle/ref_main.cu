@@ -27,6 +27,11 @@
 // order (update.cu:102-105) before the swap.  <out.mesh> receives the final
 // mask and positions.  Mesh file: uint32 magic 0x4d455348, int64 N, uint8
 // mask[N], float64 pos[N].
+//
+// With POND_REF_TIMECORR=s in the environment the driver also runs the
+// reference's TimeCorr(s) (update.cu:15-28: u *= s, T *= s*s, its call
+// commented at update.cu:123) after every step, before the swap, and scales
+// dt by s (update.cu:128).
 #include "structs.cuh"
 #include <cstdint>
 #include <cstdlib>
@@ -57,6 +62,7 @@ __global__ void cinfo_setnew_reset();
 __global__ void cinfo_set_new();
 __global__ void AMR_add();
 __global__ void AMR_remove();
+__global__ void TimeCorr(ftype dtscale);
 
 static const uint32_t MAGIC = 0x504f4e44u;
 static const uint32_t MESH_MAGIC = 0x4d455348u;
@@ -107,6 +113,8 @@ int main(int argc, char** argv) {
     return 2;
   }
   const bool mesh = argc == 8;
+  const char* tc = getenv("POND_REF_TIMECORR");
+  const double dtscale = tc ? atof(tc) : 0.0;
   const bool amr = mesh && atoi(argv[7]) != 0;
   const int nsteps = atoi(argv[3]);
   const double tau = atof(argv[4]);
@@ -220,6 +228,12 @@ int main(int argc, char** argv) {
       AMR_remove<<<1, 1>>>();
       CHECK_ERROR(cudaDeviceSynchronize());
       CHECK_ERROR(cudaGetLastError());
+    }
+    if (dtscale > 0) {  // update.cu:121-128 with the TimeCorr line enabled
+      TimeCorr<<<block, brick>>>((ftype)dtscale);
+      CHECK_ERROR(cudaDeviceSynchronize());
+      CHECK_ERROR(cudaGetLastError());
+      parsHost.dt *= dtscale;
     }
     parsHost.iStep++;
     parsHost.swapLS();

@@ -14,7 +14,8 @@ Cases with a ``scheme`` run one of the reference's alternative interpolation
 calls (steps.cu:444-463, selected by oracle/build_ref.sh's scheme argument);
 cases with a ``mesh`` also pass a node mask and node positions, and with
 ``amr`` the reference's AMR kernels run after every step; cases with
-``bc = mirror`` run the reference's disabled mirror walls.  ``--only`` makes a
+``bc = mirror`` run the reference's disabled mirror walls, and with
+``timecorr = s`` its TimeCorr(s) after every step.  ``--only`` makes a
 subset (names containing any of the given words).
 """
 from __future__ import annotations
@@ -112,9 +113,9 @@ def scheme_cases():
     cases() plus scheme, and mesh = (mask, positions, amr) for mesh runs."""
     out = []
 
-    def add(name, lat, shape, tau, nsteps, state, pseed, scheme, mesh=None, bc="periodic"):
+    def add(name, lat, shape, tau, nsteps, state, pseed, scheme, mesh=None, bc="periodic", timecorr=0.0):
         out.append(dict(name=name, lat=lat, shape=shape, tau=tau, nsteps=nsteps, state=state, pseed=pseed,
-                        scheme=scheme, mesh=mesh, bc=bc))
+                        scheme=scheme, mesh=mesh, bc=bc, timecorr=timecorr))
 
     for scheme, seed in (("lagr2", 21), ("lagr3", 22), ("lagr5", 23)):
         add(f"d1q5_{scheme}_128", 0, (128, 1, 1), 0.7, 5, smooth_state((128, 1, 1), 1, seed=seed, modes=2), seed,
@@ -133,6 +134,9 @@ def scheme_cases():
         "lagr4", bc="mirror")
     add("d3q27_mirror_8", 1, (8, 8, 8), 0.8, 2, smooth_state((8, 8, 8), 3, seed=28, modes=1, du=0.03), 28, "lagr4",
         bc="mirror")
+    # the reference's TimeCorr after every step (halving dt: u / 2, T / 4)
+    add("d1q5_timecorr_128", 0, (128, 1, 1), 0.8, 3, smooth_state((128, 1, 1), 1, seed=29, modes=2, T0=0.4), 29,
+        "lagr4", timecorr=0.5)
     return out
 
 
@@ -151,7 +155,7 @@ def cases():
 
 def all_cases():
     out = [dict(name=name, lat=lat, shape=shape, tau=tau, nsteps=nsteps, state=state, pseed=pseed, scheme="lagr4",
-                mesh=None, bc="periodic") for name, lat, shape, tau, nsteps, state, pseed in cases()]
+                mesh=None, bc="periodic", timecorr=0.0) for name, lat, shape, tau, nsteps, state, pseed in cases()]
     return out + scheme_cases()
 
 
@@ -186,7 +190,11 @@ def main():
                 min_, mout = os.path.join(td, "in.mesh"), os.path.join(td, "out.mesh")
                 write_mesh(min_, mask, pos)
                 cmd += [min_, mout, str(amr)]
-            r = subprocess.run(cmd, capture_output=True, text=True)
+            env = dict(os.environ)
+            env.pop("POND_REF_TIMECORR", None)
+            if c["timecorr"] > 0:
+                env["POND_REF_TIMECORR"] = repr(c["timecorr"])
+            r = subprocess.run(cmd, capture_output=True, text=True, env=env)
             if r.returncode != 0:
                 raise SystemExit(f"{name}: reference run failed ({r.returncode})\n{r.stdout}\n{r.stderr}")
             fo, ro, go, niter_max, ms = read_state(fout, t.Q, shape)
@@ -196,7 +204,8 @@ def main():
                              limit_lines=r.stdout.count("limit of cells division exceeded"))
         np.savez_compressed(os.path.join(args.out, name + ".npz"), lattice=lat, shape=np.array(shape), tau=tau,
                             nsteps=nsteps, f_in=f, rho_in=rho, g_in=g, f_out=fo, rho_out=ro, g_out=go,
-                            niter_max=niter_max, kernel_ms=ms, scheme=c["scheme"], bc=c["bc"], **extra)
+                            niter_max=niter_max, kernel_ms=ms, scheme=c["scheme"], bc=c["bc"],
+                            timecorr=c["timecorr"], **extra)
         print(f"{name}: NiterMax={niter_max} kernel ms/step={ms.mean():.3f}")
 
 

@@ -39,6 +39,7 @@ def replay(orc, z):
     tau = float(z["tau"])
     scheme = str(z["scheme"]) if "scheme" in z else "lagr4"
     bc = (2, 2, 2) if "bc" in z and str(z["bc"]) == "mirror" else (0, 0, 0)
+    tcorr = float(z["timecorr"]) if "timecorr" in z else 0.0
     mask = z["mask_in"].copy() if "mask_in" in z else None
     amr = int(z["amr"]) if "amr" in z else 0
     st = orc.State(z["f_in"].copy(), z["rho_in"].copy(), z["g_in"].copy())
@@ -52,6 +53,9 @@ def replay(orc, z):
         else:
             st, niter, nc = orc.step(st, lat, shape, interp=SCHEME_INTERP[scheme], tau=tau, bc=bc)
         assert nc == 0
+        if tcorr > 0:  # TimeCorr (update.cu:15-28): u *= s, T *= s*s
+            st.g[:3] *= tcorr
+            st.g[3] *= tcorr * tcorr
     return st, niter, mask
 
 
@@ -90,21 +94,21 @@ def test_mesh_file_roundtrip(tmp_path):
     assert int(raw[0]) == 0x4D455348
 
 
-@pytest.mark.parametrize("idx", range(10))
+@pytest.mark.parametrize("idx", range(11))
 def test_scheme_cases_replay_cleanly(orc, idx):
     """Every alternative-scheme and mesh case converges everywhere in the oracle,
     so a fixture made from it by the reference's kernels compares node by node."""
     from tests.golden.make_golden import scheme_cases
     from tests.states import perturbed_populations
     cases = scheme_cases()
-    assert len(cases) == 10
+    assert len(cases) == 11
     c = cases[idx]
     rho, g = c["state"]
     t = orc.tables(c["lat"])
     f = t.w[:, None] * rho[None, :] if c["pseed"] is None else perturbed_populations(orc, c["lat"], rho, g,
                                                                                       seed=c["pseed"])
     z = dict(lattice=c["lat"], shape=np.array(c["shape"]), tau=c["tau"], nsteps=c["nsteps"], f_in=f, rho_in=rho,
-             g_in=g, scheme=c["scheme"], bc=c["bc"])
+             g_in=g, scheme=c["scheme"], bc=c["bc"], timecorr=c["timecorr"])
     if c["mesh"] is not None:
         z.update(mask_in=c["mesh"][0], pos_in=c["mesh"][1], amr=c["mesh"][2])
     st, niter, mask = replay(orc, z)

@@ -187,6 +187,10 @@ def test_matches_reference_fixtures_directly(pond):
                 m = s.get_mask()
                 assert np.array_equal(m, z["mask_out"]), os.path.basename(p)
                 sel = m == 1
+            elif "timecorr" in z.files and float(z["timecorr"]) > 0:
+                for _ in range(int(z["nsteps"])):
+                    s.step(1)
+                    s.rescale_time(float(z["timecorr"]))
             else:
                 s.step(int(z["nsteps"]))
             f, rho, g = s.get_state()
