@@ -123,6 +123,8 @@ def scheme_cases():
     add("d1q5_weno5_sod_128", 0, (128, 1, 1), 0.55, 6, sod_state(128, (1.0, 0.0, 0.01), (0.125, 0.0, 0.008)), None,
         "weno5")
     add("d3q27_lagr3_8", 1, (8, 8, 8), 0.8, 2, smooth_state((8, 8, 8), 3, seed=24, modes=1, du=0.03), 24, "lagr3")
+    add("d3q27_lagr2_8", 1, (8, 8, 8), 0.8, 2, smooth_state((8, 8, 8), 3, seed=30, modes=1, du=0.03), 30, "lagr2")
+    add("d3q27_lagr5_8", 1, (8, 8, 8), 0.8, 2, smooth_state((8, 8, 8), 3, seed=31, modes=1, du=0.03), 31, "lagr5")
     add("d1q5_gap2_mask_128", 0, (128, 1, 1), 0.7, 4, smooth_state((128, 1, 1), 1, seed=25, modes=2), 25, "gap2",
         (sparse_mask(128, 25), np.arange(128, dtype=np.float64), 0))
     add("d1q5_gap2_amr_sod_128", 0, (128, 1, 1), 0.6, 6, sod_state(128, (1.0, 0.0, 0.01), (0.125, 0.0, 0.008)),
