@@ -125,6 +125,10 @@ int pond_create(const pond_params* params, pond_ctx** out);
 int pond_destroy(pond_ctx* ctx);
 int pond_get_params(const pond_ctx* ctx, pond_params* out);
 int pond_q(int lattice);
+/* lattice tables in the reference's population order (consts.h): xi[3*Q]
+   velocity components of each population at T = TLat (ef, or e for D3Q27),
+   w[Q] weights, tlat_dim[2] = {TLat, Dim}; any pointer may be NULL.  Host only. */
+int pond_lattice_tables(int lattice, double* xi, double* w, double* tlat_dim);
 
 /* ic_params: ACOUSTIC {T0, amplitude, gamma}; SOD_X {x0, rhoL, uL, TL, rhoR, uR, TR};
    SPHERE {cx, cy, cz, radius, rho_in, T_in, rho_out, T_out};

@@ -26,7 +26,7 @@ from ._lib import (BC_CLAMP, BC_MIRROR, BC_PERIODIC, D1Q5, D3Q27, D3Q125, FIXED3
                    IC_SOD_X, IC_SPHERE, IC_TGV, IC_UNIFORM, LAGR2, LAGR3, LAGR4, LAGR5, NONUNIFORM3, TVD, WENO5,
                    PondError)
 
-__all__ = ["Solver", "PondError", "lattice_q", "D1Q5", "D3Q27", "D3Q125", "LAGR2", "LAGR3", "LAGR4", "LAGR5",
+__all__ = ["Solver", "PondError", "lattice_q", "lattice_tables", "D1Q5", "D3Q27", "D3Q125", "LAGR2", "LAGR3", "LAGR4", "LAGR5",
            "FIXED3", "TVD", "WENO5", "GAP2", "NONUNIFORM3", "BC_PERIODIC", "BC_CLAMP", "BC_MIRROR", "FP32", "FP64",
            "IC_ACOUSTIC", "IC_SOD_X", "IC_SPHERE", "IC_TGV", "IC_UNIFORM", "write_arr", "read_arr"]
 
@@ -42,6 +42,18 @@ def _dp(a):
 def lattice_q(lattice) -> int:
     lat = _LATTICES.get(lattice, lattice)
     return _lib.load().pond_q(int(lat))
+
+
+def lattice_tables(lattice):
+    """(xi[Q, 3], w[Q], TLat, Dim) in the reference's population order (consts.h)."""
+    lat = int(_LATTICES.get(lattice, lattice))
+    L = _lib.load()
+    Q = L.pond_q(lat)
+    if Q <= 0:
+        raise ValueError(f"unknown lattice {lattice}")
+    xi, w, td = np.zeros(3 * Q), np.zeros(Q), np.zeros(2)
+    _lib.check(L.pond_lattice_tables(lat, _dp(xi), _dp(w), _dp(td)))
+    return xi.reshape(Q, 3), w, float(td[0]), float(td[1])
 
 
 class Solver:
@@ -273,8 +285,22 @@ class Solver:
         _lib.check(self._L.pond_device_state(self._ctx, ctypes.byref(f), ctypes.byref(r), ctypes.byref(g)))
         return f.value, r.value, g.value
 
-    def drop(self, directory: str):
-        """Write Rho/Vx/Vy/Vz/T_%07d.arr for the current step (drop.cu:2-34)."""
+    def draw_fields(self, names=None) -> dict:
+        """The viewer's per-node fields (lbm_draw, lbm.cu:30-73; see
+        lbmpond_b200.fields): rho, ux, mach, T, M4, f0..f8 by default, and
+        "niter" when named (it needs keep_niter(True) before the last step)."""
+        from .fields import FIELD_NAMES, draw_fields
+        names = tuple(n for n in FIELD_NAMES if n != "niter") if names is None else tuple(names)
+        f, rho, g = self.get_state()
+        xi, _, tlat, _ = lattice_tables(self.lattice)
+        niter = self.niter() if "niter" in names else None
+        mask = self.get_mask() if self.params.interp in (GAP2, NONUNIFORM3) else None
+        return draw_fields(f, rho, g, xi[:, 0], tlat, dt=self.dt, niter=niter, mask=mask, names=names)
+
+    def drop(self, directory: str, fields=()):
+        """Write Rho/Vx/Vy/Vz/T_%07d.arr for the current step (drop.cu:2-34),
+        and one <Name>_%07d.arr per extra viewer field in `fields` (names of
+        draw_fields, e.g. ("mach", "M4"))."""
         fl = self.fields()
         istep = self.diagnostics()["istep"]
         os.makedirs(directory, exist_ok=True)
@@ -284,6 +310,11 @@ class Solver:
             path = os.path.join(directory, f"{prefix}_{istep:07d}.arr")
             write_arr(path, fl[key], self.shape)
             paths.append(path)
+        if fields:
+            for key, data in self.draw_fields(fields).items():
+                path = os.path.join(directory, f"{key[0].upper() + key[1:]}_{istep:07d}.arr")
+                write_arr(path, data, self.shape)
+                paths.append(path)
         return paths
 
 

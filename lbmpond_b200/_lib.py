@@ -57,6 +57,7 @@ SIGNATURES = {
     "pond_destroy": (ctypes.c_int, [_vp]),
     "pond_get_params": (ctypes.c_int, [_vp, ctypes.POINTER(PondParams)]),
     "pond_q": (ctypes.c_int, [ctypes.c_int]),
+    "pond_lattice_tables": (ctypes.c_int, [ctypes.c_int, _dp, _dp, _dp]),
     "pond_init": (ctypes.c_int, [_vp, ctypes.c_int, _dp, ctypes.c_int]),
     "pond_set_state": (ctypes.c_int, [_vp, _dp, _dp, _dp]),
     "pond_get_state": (ctypes.c_int, [_vp, _dp, _dp, _dp]),

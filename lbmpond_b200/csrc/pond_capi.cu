@@ -57,6 +57,22 @@ double lattice_weight_host(int lattice, int ref_index) {
 }
 
 double lattice_tlat(int lattice) { return lattice == POND_D3Q27 ? 1.0 / 3.0 : 1.0; }
+
+// velocities and weights of every population in the reference's order
+template <int LAT> static void tables_of(double* xi, double* w) {
+  using L = Lattice<LAT>;
+  for (int t = 0; t < L::Q; t++) {  // tensor class t -> reference population ref(cx, cy, cz)
+    const int cx = L::D == 1 ? t : t / (L::Q1 * L::Q1);
+    const int cy = L::D == 1 ? 0 : (t / L::Q1) % L::Q1, cz = L::D == 1 ? 0 : t % L::Q1;
+    const int q = L::ref(cx, cy, cz);
+    if (xi) {
+      xi[3 * q] = L::xi1(cx);
+      xi[3 * q + 1] = L::D == 1 ? 0.0 : L::xi1(cy);
+      xi[3 * q + 2] = L::D == 1 ? 0.0 : L::xi1(cz);
+    }
+    if (w) w[q] = lattice_weight_t<LAT>(t);
+  }
+}
 double lattice_dim(int lattice) { return lattice == POND_D1Q5 ? 1.0 : 3.0; }
 
 bool scheme_supported(int lattice, int interp) {
@@ -184,6 +200,17 @@ const char* pond_status_string(int s) {
 const char* pond_last_error_string(void) { return g_last_error.c_str(); }
 
 int pond_q(int lattice) { return lattice_q(lattice); }
+
+int pond_lattice_tables(int lattice, double* xi, double* w, double* tlat_dim) {
+  switch (lattice) {
+    case POND_D1Q5: tables_of<POND_D1Q5>(xi, w); break;
+    case POND_D3Q27: tables_of<POND_D3Q27>(xi, w); break;
+    case POND_D3Q125: tables_of<POND_D3Q125>(xi, w); break;
+    default: return set_error(POND_ERR_ARG, "unknown lattice %d", lattice);
+  }
+  if (tlat_dim) { tlat_dim[0] = lattice_tlat(lattice); tlat_dim[1] = lattice_dim(lattice); }
+  return POND_OK;
+}
 
 int pond_params_default(int lattice, pond_params* out) {
   if (!out) return set_error(POND_ERR_ARG, "pond_params_default: null output");
