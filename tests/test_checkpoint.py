@@ -1,7 +1,8 @@
 """Checkpoint / resume (lbmpond_b200.checkpoint) on the CPU: the file format,
 the Solver arguments it recreates, and the order in which a resume loads the
 state.  A stand-in object plays the CUDA context; the GPU round trip (a
-resumed context stepping bit for bit like the original) needs a device."""
+resumed context stepping bit for bit like the original) is in
+tests/test_zy_api_gpu.py."""
 import ctypes
 
 import numpy as np
@@ -99,31 +100,3 @@ def test_set_clock_validates_before_device(pond):
     L = _lib.load()
     assert L.pond_set_clock(None, 1, 0.0, 1.0) == -1
 
-
-@pytest.mark.gpu
-@pytest.mark.parametrize("interp,precision", [(4, "fp32"), (4, "fp64"), (9, "fp32"), (10, "fp64")])
-def test_resumed_context_continues_the_run(tmp_path, pond, interp, precision):
-    """Checkpoint after 3 steps, 2 more steps on the original and on a context
-    resumed from the file: the same state bit for bit, the same clock."""
-    nx = 64
-    with pond.Solver(lattice="D1Q5", shape=(nx, 1, 1), interp=interp, precision=precision, tau=0.7, dt=0.5) as s:
-        s.init("sod")
-        if interp == 9:
-            s.set_mask(np.arange(nx) % 3 != 1)
-        if interp == 10:
-            s.set_positions(np.arange(nx) + 0.2 * np.sin(2 * np.pi * np.arange(nx) / nx))
-        s.step(3)
-        path = str(tmp_path / "run.npz")
-        s.checkpoint(path)
-        s.step(2)
-        a, da = s.get_state(), s.diagnostics()
-    with pond.Solver.resume(path) as r:
-        assert r.diagnostics()["istep"] == 3 and r.dt == 0.5
-        r.step(2)
-        b, db = r.get_state(), r.diagnostics()
-        if interp in (9, 10):
-            assert r.get_mask().sum() == (nx - nx // 3 if interp == 9 else nx)
-    for x, y in zip(a, b):
-        assert np.array_equal(x, y)
-    assert db["istep"] == da["istep"] == 5 and db["curtime"] == da["curtime"] == 2.5
-    assert np.isclose(db["mass"], da["mass"], rtol=1e-14)

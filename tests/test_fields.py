@@ -1,7 +1,6 @@
 """The viewer's derived fields (lbmpond_b200.fields, lbm_draw lbm.cu:30-73) and
-the library's lattice tables, on the CPU; one GPU test reads them off a
-stepped context."""
-import ctypes
+the library's lattice tables, on the CPU (the GPU test that reads them off a
+stepped context is in tests/test_zy_api_gpu.py)."""
 
 import numpy as np
 import pytest
@@ -58,26 +57,3 @@ def test_mask_and_niter():
     with pytest.raises(ValueError):
         draw_fields(f, rho, g, xi, 1.0, names=("vorticity",))
 
-
-@pytest.mark.gpu
-def test_solver_draw_fields_and_drop(tmp_path, pond):
-    nx = 64
-    with pond.Solver(lattice="D1Q5", shape=(nx, 1, 1), interp=pond.GAP2, precision="fp64", tau=0.7, dt=0.5) as s:
-        s.init("sod")
-        s.set_mask(np.arange(nx) % 4 != 2)
-        s.keep_niter(True)
-        s.step(2)
-        out = s.draw_fields(FIELD_NAMES)
-        f, rho, g = s.get_state()
-        mask, niter = s.get_mask(), s.niter()
-        xi, _, tlat, _ = pond.lattice_tables("D1Q5")
-        expect = draw_fields(f, rho, g, xi[:, 0], tlat, dt=0.5, niter=niter, mask=mask)
-        for name in FIELD_NAMES:
-            assert np.array_equal(out[name], expect[name]), name
-        assert out["niter"][mask == 1].min() >= 1
-        paths = s.drop(str(tmp_path), fields=("mach", "M4"))
-    names = sorted(p.rsplit("/", 1)[1] for p in paths)
-    assert names == ["M4_0000002.arr", "Mach_0000002.arr", "Rho_0000002.arr", "T_0000002.arr",
-                     "Vx_0000002.arr", "Vy_0000002.arr", "Vz_0000002.arr"]
-    data, shape = pond.read_arr(str(tmp_path / "Mach_0000002.arr"))
-    assert shape == (nx, 1, 1) and np.allclose(data, expect["mach"], equal_nan=True)
