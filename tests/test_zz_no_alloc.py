@@ -92,3 +92,48 @@ def test_noalloc_rejects_grids_beyond_its_scratch(pond):
     st = step_noalloc(ctypes.byref(p), one, one, one, one, one, one, one, None)
     assert st == -1
     assert "scratch" in L.pond_last_error_string().decode()
+
+
+def test_noalloc_step_leaves_guard_bands_untouched(orc, pond):
+    """Guard-band canaries around every caller-owned array: each plane set
+    sits inside a larger allocation whose first and last 1024 elements (4 KB,
+    keeping every interior pointer 16-byte aligned) hold a sentinel pattern;
+    after two steps the bands are bit for bit unchanged and every output value
+    is finite."""
+    import torch
+    from lbmpond_b200 import _lib
+    L = _lib.load()
+    step_noalloc = _bind(L)
+    shape = (40, 12, 6)
+    N = int(np.prod(shape))
+    rho, g = smooth_state(shape, 3, seed=22, modes=1, du=0.03)
+    f = perturbed_populations(orc, 1, rho, g, seed=22, eps=0.01)
+    p = _lib.PondParams()
+    assert L.pond_params_default(1, ctypes.byref(p)) == 0
+    p.Nx, p.Ny, p.Nz = shape
+    p.tau = 0.8
+    dev = torch.device("cuda", 0)
+    G = 1024
+    sentinel = torch.tensor([-1.234567e30], dtype=torch.float32).view(torch.int32).item()
+
+    def guarded(host):
+        n = host.size
+        t = torch.full((n + 2 * G,), sentinel, dtype=torch.int32, device=dev).view(torch.float32)
+        t[G:G + n] = torch.from_numpy(host.astype(np.float32).ravel()).to(dev)
+        return t, n
+
+    sets = [[guarded(a) for a in (f, rho, g)] for _ in range(2)]
+    diag = torch.zeros(ctypes.sizeof(_lib.PondDiag), dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    for call in range(2):
+        src, dst = sets[call % 2], sets[(call + 1) % 2]
+        ptrs = [t.data_ptr() + 4 * G for t, _ in src] + [t.data_ptr() + 4 * G for t, _ in dst]
+        st = step_noalloc(ctypes.byref(p), *ptrs, diag.data_ptr(), stream)
+        assert st == 0, L.pond_last_error_string().decode()
+    torch.cuda.synchronize(dev)
+    for group in sets:
+        for t, n in group:
+            bits = t.view(torch.int32)
+            assert bool((bits[:G] == sentinel).all()) and bool((bits[G + n:] == sentinel).all())
+            assert bool(torch.isfinite(t[G:G + n]).all())
+    assert N == sets[0][1][1]
