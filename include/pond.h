@@ -41,7 +41,7 @@ typedef enum {
   POND_ERR_NOMEM = -3,        /* device allocation failed */
   POND_ERR_STATE = -4,        /* call out of order (e.g. step before init) */
   POND_ERR_UNSUPPORTED = -5,  /* lattice / scheme / precision combination not built */
-  POND_ERR_NOT_CONVERGED = -6 /* reserved for callers that treat max_iter hits as errors */
+  POND_ERR_NOT_CONVERGED = -6 /* a node reached max_iter (only with pond_set_strict) */
 } pond_status;
 
 /* lattices: consts.h:6-12 picks one at compile time; here it is a parameter */
@@ -149,6 +149,11 @@ int pond_get_fields(pond_ctx* ctx, double* rho, double* ux, double* uy, double* 
 /* advance nsteps steps (calcStep without drop/diagnostics printing) */
 int pond_step(pond_ctx* ctx, int nsteps);
 int pond_diagnostics(pond_ctx* ctx, pond_diag* out);
+/* strict = 1: pond_step reads each step's counters back and returns
+   POND_ERR_NOT_CONVERGED after the first step that left a node at max_iter
+   (that step is complete and counted; the reference prints NiterMax and goes
+   on, update.cu:131).  strict = 0 (default): the count is in pond_diagnostics. */
+int pond_set_strict(pond_ctx* ctx, int strict);
 /* the step counter, simulated time and dt of a resumed run (LBMParamsHost
    iStep / curtime / dt); dt <= 0 keeps the current dt.  Host bookkeeping only. */
 int pond_set_clock(pond_ctx* ctx, int64_t istep, double curtime, double dt);

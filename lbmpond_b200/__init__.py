@@ -217,6 +217,10 @@ class Solver:
         _lib.check(self._L.pond_get_params(self._ctx, ctypes.byref(p)))
         return p
 
+    def set_strict(self, on=True):
+        """Make step() raise PondError (status -6) after a step that left nodes at max_iter."""
+        _lib.check(self._L.pond_set_strict(self._ctx, 1 if on else 0))
+
     def set_clock(self, istep, curtime, dt=0.0):
         """Step counter, simulated time and (if > 0) dt of a resumed run."""
         _lib.check(self._L.pond_set_clock(self._ctx, int(istep), float(curtime), float(dt)))

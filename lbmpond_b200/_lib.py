@@ -67,6 +67,7 @@ SIGNATURES = {
     "pond_step": (ctypes.c_int, [_vp, ctypes.c_int]),
     "pond_diagnostics": (ctypes.c_int, [_vp, ctypes.POINTER(PondDiag)]),
     "pond_set_clock": (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.c_double, ctypes.c_double]),
+    "pond_set_strict": (ctypes.c_int, [_vp, ctypes.c_int]),
     "pond_keep_niter": (ctypes.c_int, [_vp, ctypes.c_int]),
     "pond_get_niter": (ctypes.c_int, [_vp, _i32p]),
     "pond_keep_history": (ctypes.c_int, [_vp, ctypes.c_int]),

@@ -522,6 +522,17 @@ int pond_step(pond_ctx* c, int nsteps) {
       st = dt_adapt_after_step(c);
       if (st != POND_OK) return st;
     }
+    if (c->strict) {
+      e = cudaMemcpyAsync(c->h_sums, c->d_sums, sizeof(StepSums), cudaMemcpyDeviceToHost, c->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+      if (e != cudaSuccess) return cuda_fail(e, "sums download");
+      c->have_sums = true;
+      if (c->h_sums->nonconv) {
+        cudaEventRecord(c->ev1, c->stream);
+        return set_error(POND_ERR_NOT_CONVERGED, "step %lld: %llu nodes reached max_iter = %d", c->istep,
+                         (unsigned long long)c->h_sums->nonconv, c->p.max_iter);
+      }
+    }
   }
   e = cudaEventRecord(c->ev1, c->stream);
   if (e != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
@@ -637,6 +648,12 @@ int pond_last_step_work(pond_ctx* c, int64_t* work) {
   cudaError_t e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_fail(e, "pond_last_step_work");
   *work = c->have_sums ? (int64_t)c->h_sums->work : 0;
+  return POND_OK;
+}
+
+int pond_set_strict(pond_ctx* c, int strict) {
+  if (!c) return set_error(POND_ERR_ARG, "null context");
+  c->strict = strict != 0;
   return POND_OK;
 }
 

@@ -57,6 +57,7 @@ struct pond_ctx {
   uint8_t* amr_sigma = nullptr;           // coarsening: automaton state entering each chunk
   unsigned long long* amr_counts = nullptr;  // [4] device counters
   unsigned long long* amr_counts_h = nullptr;  // pinned copy
+  bool strict = false;  // pond_step stops with POND_ERR_NOT_CONVERGED after a step with nodes at max_iter
   // time-step adaptation after every step (update.cu:121-123)
   bool dt_adapt = false;
   int adapt_hi = 1000, adapt_lo = 4;

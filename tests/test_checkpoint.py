@@ -99,4 +99,6 @@ def test_read_rejects_other_files(tmp_path):
 def test_set_clock_validates_before_device(pond):
     L = _lib.load()
     assert L.pond_set_clock(None, 1, 0.0, 1.0) == -1
+    assert L.pond_set_strict(None, 1) == -1
+    assert L.pond_status_string(-6).decode() == "iteration did not converge"
 

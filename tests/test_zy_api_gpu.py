@@ -1,6 +1,7 @@
 """API round trips on the GPU, through the C ABI: a context resumed from a
-checkpoint continues the run bit for bit, and the viewer's derived fields and
-.arr files of a stepped context equal the host formulas applied to its state.
+checkpoint continues the run bit for bit, the viewer's derived fields and
+.arr files of a stepped context equal the host formulas applied to its state,
+and the strict mode turns an iteration-cap hit into an error status.
 These exercise the host-side API around the step; the step's own parity with
 the oracle is in the test_gpu_* files."""
 import numpy as np
@@ -60,3 +61,27 @@ def test_solver_draw_fields_and_drop(tmp_path, pond):
                      "Vx_0000002.arr", "Vy_0000002.arr", "Vz_0000002.arr"]
     data, shape = pond.read_arr(str(tmp_path / "Mach_0000002.arr"))
     assert shape == (nx, 1, 1) and np.allclose(data, expect["mach"], equal_nan=True)
+
+
+@pytest.mark.gpu
+def test_strict_mode_reports_nonconvergence(pond):
+    """With pond_set_strict a step that leaves nodes at max_iter returns
+    POND_ERR_NOT_CONVERGED (the step itself is complete and counted); without
+    it the same step succeeds and the count is in the diagnostics."""
+    nx = 32
+    kw = dict(lattice="D1Q5", shape=(nx, 1, 1), precision="fp64", tau=0.8, max_iter=1)
+    with pond.Solver(**kw) as s:
+        s.init("sod")
+        s.step(1)
+        assert s.diagnostics()["nonconverged"] > 0
+    with pond.Solver(**kw) as s:
+        s.init("sod")
+        s.set_strict(True)
+        with pytest.raises(pond.PondError) as e:
+            s.step(3)
+        assert e.value.status == -6
+        d = s.diagnostics()
+        assert d["istep"] == 1 and d["nonconverged"] > 0
+        s.set_strict(False)
+        s.step(1)
+        assert s.diagnostics()["istep"] == 2
