@@ -219,3 +219,42 @@ def test_mesh_step_rejects_walls(orc):
     nc = orc.lib().orc_step_mesh(ctypes.byref(p), orc._dp(st.f), orc._dp(st.rho), orc._dp(st.g), None, None,
                                  *[orc._dp(a) for a in out], None)
     assert nc < 0
+
+
+def test_amr_sod_characterisation(orc):
+    """The reference's AMR on a periodic Sod tube (400 nodes, gamma 3, tau
+    0.55, 120 steps, GAP2), started on every other node with refinement and
+    coarsening after every step: it keeps well under half the nodes active
+    and stays within a few percent (L1 in rho, central half, away from the
+    seam's second jump) of the exact solution, coarser than the full grid."""
+    from tests.riemann import sample
+    nx, steps, lam2 = 400, 120, 0.01
+    x = np.arange(nx)
+    left, right = (1.0, 0.0, lam2), (0.125, 0.0, lam2 * 0.1 / 0.125)
+    rho = np.where(x < nx // 2, left[0], right[0])
+    g = np.stack([np.zeros(nx), np.zeros(nx), np.zeros(nx), np.where(x < nx // 2, left[2], right[2])])
+    t = orc.tables(0)
+    st0 = orc.State(t.w[:, None] * rho[None, :], rho.copy(), g)
+    er = sample((left[0], 0.0, left[0] * left[2]), (right[0], 0.0, right[0] * right[2]), 3.0,
+                (x - (nx / 2 - 0.5)) / steps)[0]
+    mid = (x > nx * 0.25) & (x < nx * 0.75)
+
+    def l1(st, mask):
+        m = mid & (mask == 1)
+        return float(np.abs(st.rho[m] - er[m]).mean() / er[m].mean())
+
+    st = st0.copy()
+    for _ in range(steps):
+        st, _, nc = orc.step_mesh(st, nx, interp=orc.GAP2, tau=0.55)
+        assert nc == 0
+    full = l1(st, np.ones(nx, np.uint8))
+    st, mask, active = st0.copy(), (x % 2 == 0).astype(np.uint8), []
+    for _ in range(steps):
+        st, _, nc = orc.step_mesh(st, nx, interp=orc.GAP2, mask=mask, tau=0.55)
+        assert nc == 0
+        st, mask, _, _ = orc.amr_refine(st, mask, 0.01)
+        mask, _ = orc.amr_coarsen(st, mask, 0.01)
+        active.append(int(mask.sum()))
+    amr = l1(st, mask)
+    assert full < 0.02 and full < amr < 0.05, (full, amr)
+    assert 90 < min(active) and max(active) < 200, (min(active), max(active))
