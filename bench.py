@@ -588,6 +588,11 @@ def run_mesh1d(steps=20, warmup=3, n=1 << 24):
     except OSError:
         pass
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    measured = {}
+    try:  # DRAM bytes per grid node of each kernel, from one ncu capture (profiles/pull_1d_mesh_4M.md)
+        measured = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+    except OSError:
+        pass
     out = {"workload": f"D1Q5 Sod tube, {n} nodes, float32, tau 0.55, periodic", "steps": steps, "warmup": warmup}
     sod = (0.5, 1.0, 0.0, 0.01, 0.125, 0.0, 0.008)
     for scheme in ("GAP2", "NONUNIFORM3"):
@@ -612,10 +617,12 @@ def run_mesh1d(steps=20, warmup=3, n=1 << 24):
                 rec["coarsen_ms"] = (time.perf_counter() - t0) * 1e3
                 rec["coarsened_nodes"] = removed
             gbs = 56.0 * active / (ms / 1e3) / 1e9
+            t = measured.get("pull_1d_mesh_" + ("gap2" if scheme == "GAP2" else "nu3") + "_f32")
             rec.update({"active_nodes": active, "ms_per_step": ms, "MLUPS": active / (ms / 1e3) / 1e6,
                         "niter_mean": d["niter_mean"], "niter_max": d["niter_max"],
                         "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm_peak, "unit": "GB/s",
-                                     "frac": gbs / hbm_peak, "bytes_per_node": 56}})
+                                     "frac": gbs / hbm_peak, "bytes_per_node": 56,
+                                     "traffic": t["bytes_per_node"] * n if t else None}})
             out[scheme.lower()] = rec
     return out
 
