@@ -17,13 +17,13 @@
 # Only comment markers and the template argument change; the binary name
 # carries the scheme unless it is lagr4.
 #
-# bc = mirror sets the `outflow` flags of steps.cu; on the D1Q5 / D3Q27 path
-# only propagate<N>'s counts (steps.cu:1004-1013): the stencil is reflected
-# at every face with the populations reversed (Cell::mirrX/Y/Z,
-# structs.cuh:552-578).  periodic (default) leaves them off.  With the
-# Lagrange schemes only (the other propagators never read the flag), and not
-# on D3Q125, whose flag (steps.cu:373) moves x positions without reversing
-# populations.
+# bc = mirror sets the `outflow` flags of steps.cu.  On the D1Q5 / D3Q27
+# path only propagate<N>'s counts (steps.cu:1004-1013): the stencil is
+# reflected at every face with the populations reversed and u negated
+# (Cell::mirrX/Y/Z, structs.cuh:552-578).  On D3Q125 only the launched
+# PonDstepD3Q125's counts (steps.cu:167-191): the same reflection through
+# the reverse tables.  periodic (default) leaves them off.  With the
+# Lagrange schemes only (the other propagators never read the flag).
 #
 # The reference sources stay where they are (read-only); patched copies live
 # in a temporary directory and only the binary is written, into oracle/_ref/.
@@ -42,8 +42,7 @@ OUT="$HERE/_ref"
 LAT=${1:?lattice}; PREC=${2:?precision}; NX=${3:?nx}; NY=${4:?ny}; NZ=${5:?nz}; SCHEME=${6:-lagr4}; BC=${7:-periodic}
 case "$BC" in
   periodic) ;;
-  mirror) [ "$LAT" != D3Q125 ] || { echo "mirror: D1Q5 and D3Q27 only" >&2; exit 2; }
-          case "$SCHEME" in lagr*) ;; *) echo "mirror: Lagrange schemes only" >&2; exit 2;; esac ;;
+  mirror) case "$SCHEME" in lagr*) ;; *) echo "mirror: Lagrange schemes only" >&2; exit 2;; esac ;;
   *) echo "bad bc $BC" >&2; exit 2;;
 esac
 case "$SCHEME" in lagr2|lagr3|lagr4|lagr5|weno5|gap2|nu3) ;; *) echo "bad scheme $SCHEME" >&2; exit 2;; esac

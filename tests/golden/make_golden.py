@@ -136,6 +136,8 @@ def scheme_cases():
         "lagr4", bc="mirror")
     add("d3q27_mirror_8", 1, (8, 8, 8), 0.8, 2, smooth_state((8, 8, 8), 3, seed=28, modes=1, du=0.03), 28, "lagr4",
         bc="mirror")
+    add("d3q125_mirror_8x4x4", 2, (8, 4, 4), 0.9, 2, smooth_state((8, 4, 4), 3, seed=32, modes=1, du=0.02), 32,
+        "lagr4", bc="mirror")
     # the reference's TimeCorr after every step (halving dt: u / 2, T / 4)
     add("d1q5_timecorr_128", 0, (128, 1, 1), 0.8, 3, smooth_state((128, 1, 1), 1, seed=29, modes=2, T0=0.4), 29,
         "lagr4", timecorr=0.5)
