@@ -292,7 +292,11 @@ int pond_predict(pond_ctx* ctx, float* guess);
    to diag_out, a pond_diag in DEVICE memory; istep and curtime are left 0.
    Work is queued on `stream` (a cudaStream_t, 0 = legacy default stream); the
    call does not synchronise.  params->device is ignored: the current device
-   is used.
+   is used.  The six state buffers must be pairwise disjoint (an output that
+   overlaps an input or another output is rejected with POND_ERR_ARG: the
+   step reads neighbours of the input while other CTAs write the output).
+   params->learned and params->ddf must be 0 (POND_ERR_UNSUPPORTED); tau,
+   max_iter (1..100000) and the tolerances are checked as in pond_create.
 
    It is meant for callers that cannot let a library call cudaMalloc: code
    that owns all device memory through its own pool or a budget fixed at
@@ -306,7 +310,9 @@ int pond_predict(pond_ctx* ctx, float* guess);
    up that array's device address (and opts the kernel into its shared
    memory); make that first call before any stream capture.  All calls share
    the array and every call rewrites it: calls whose kernels overlap on a GPU
-   (other streams, other threads) race on it. */
+   (other streams, other threads) race on it, so serialise them on one stream.
+   The looked-up address is kept for the life of the process: do not call
+   cudaDeviceReset on a device between calls of this entry point. */
 #define POND_NOALLOC_SCRATCH_BYTES 5242880
 int pond_step_noalloc(const pond_params* params, const float* f_in, const float* rho_in, const float* g_in,
                       float* f_out, float* rho_out, float* g_out, pond_diag* diag_out, void* stream);

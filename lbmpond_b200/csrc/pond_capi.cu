@@ -75,6 +75,19 @@ template <int LAT> static void tables_of(double* xi, double* w) {
 }
 double lattice_dim(int lattice) { return lattice == POND_D1Q5 ? 1.0 : 3.0; }
 
+// Checks shared by every entry point that runs a step from a pond_params:
+// boundaries, tau, the iteration cap and the tolerances.  The cap bounds the
+// length of one step launch on a shared GPU.
+int check_step_params(const pond_params* p) {
+  for (int a = 0; a < 3; a++)
+    if (p->bc[a] < POND_BC_PERIODIC || p->bc[a] > POND_BC_MIRROR) return set_error(POND_ERR_ARG, "bad bc[%d]", a);
+  if (!(p->tau > 0.5) || !std::isfinite(p->tau)) return set_error(POND_ERR_ARG, "tau must be a finite value > 0.5");
+  if (p->max_iter < 1 || p->max_iter > 100000) return set_error(POND_ERR_ARG, "max_iter out of range (1..100000)");
+  if (!(p->tol_abs >= 0) || !(p->tol_rel >= 0) || !std::isfinite(p->tol_abs) || !std::isfinite(p->tol_rel))
+    return set_error(POND_ERR_ARG, "tolerances must be finite and >= 0");
+  return POND_OK;
+}
+
 bool scheme_supported(int lattice, int interp) {
   switch (lattice) {
     case POND_D1Q5:
@@ -245,11 +258,8 @@ int pond_create(const pond_params* p, pond_ctx** out) {
     return set_error(POND_ERR_ARG, "unknown precision %d", p->precision);
   if (!scheme_supported(p->lattice, p->interp))
     return set_error(POND_ERR_UNSUPPORTED, "interpolation %d is not available for lattice %d", p->interp, p->lattice);
-  for (int a = 0; a < 3; a++)
-    if (p->bc[a] < POND_BC_PERIODIC || p->bc[a] > POND_BC_MIRROR) return set_error(POND_ERR_ARG, "bad bc[%d]", a);
-  if (!(p->tau > 0.5) || !std::isfinite(p->tau)) return set_error(POND_ERR_ARG, "tau must be a finite value > 0.5");
-  if (p->max_iter < 1 || p->max_iter > 100000) return set_error(POND_ERR_ARG, "max_iter out of range");
-  if (!(p->tol_abs >= 0) || !(p->tol_rel >= 0)) return set_error(POND_ERR_ARG, "tolerances must be >= 0");
+  const int vst = check_step_params(p);
+  if (vst != POND_OK) return vst;
   if (p->lattice == POND_D1Q5 && (p->interp == POND_TVD || p->interp == POND_WENO5) && (p->Ny != 1 || p->Nz != 1))
     return set_error(POND_ERR_UNSUPPORTED, "TVD/WENO5 run on 1D grids (Ny = Nz = 1)");
   if (p->lattice == POND_D1Q5 && mesh_scheme(p->interp)) {

@@ -67,6 +67,8 @@ namespace pond {
 int set_error(int status, const char* fmt, ...);
 int cuda_fail(cudaError_t e, const char* what);
 int lattice_q(int lattice);
+// boundaries, tau, max_iter and tolerances of a step's parameters (POND_OK or POND_ERR_ARG)
+int check_step_params(const pond_params* p);
 double lattice_weight_host(int lattice, int ref_index);
 double lattice_tlat(int lattice);
 double lattice_dim(int lattice);

@@ -19,6 +19,7 @@
 // overlap on a GPU (different streams, or threads) race on it.
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <mutex>
 
 #include "pond_internal.h"
@@ -77,6 +78,25 @@ __global__ void __launch_bounds__(256) reduce_partials_kernel(const d27::BlockPa
   }
 }
 
+// The step reads neighbouring nodes of f_in/rho_in/g_in while other CTAs
+// write f_out/rho_out/g_out, so every output range (27 N, N and 4 N floats)
+// must be disjoint from every input range and from the other outputs.
+static bool any_overlap(long long N, const float* fi, const float* ri, const float* gi, const float* fo,
+                        const float* ro, const float* go) {
+  struct Range { uintptr_t lo, hi; };
+  auto rg = [](const float* p, long long n) { return Range{(uintptr_t)p, (uintptr_t)p + (uintptr_t)n * 4u}; };
+  const Range in[3] = {rg(fi, 27 * N), rg(ri, N), rg(gi, 4 * N)};
+  const Range out[3] = {rg(fo, 27 * N), rg(ro, N), rg(go, 4 * N)};
+  auto meet = [](Range a, Range b) { return a.lo < b.hi && b.lo < a.hi; };
+  for (int o = 0; o < 3; o++) {
+    for (int i = 0; i < 3; i++)
+      if (meet(out[o], in[i])) return true;
+    for (int j = o + 1; j < 3; j++)
+      if (meet(out[o], out[j])) return true;
+  }
+  return false;
+}
+
 // Once per device: the scratch array's device address and the step kernels'
 // shared-memory opt-in.  Called with the target device current.
 static int setup_device(void** addr) {
@@ -116,14 +136,13 @@ extern "C" int pond_step_noalloc(const pond_params* p, const float* f_in, const 
   if (p->lattice != POND_D3Q27 || p->precision != POND_FP32 || p->interp < POND_LAGR2 || p->interp > POND_LAGR4)
     return set_error(POND_ERR_UNSUPPORTED, "pond_step_noalloc runs D3Q27, float32, Lagrange order 2-4 only");
   if (p->ddf) return set_error(POND_ERR_UNSUPPORTED, "pond_step_noalloc carries no energy populations");
+  if (p->learned) return set_error(POND_ERR_UNSUPPORTED, "pond_step_noalloc has no learned start (learned = 0)");
   if (p->Nx <= 0 || p->Ny <= 0 || p->Nz <= 0 || p->Nx > (1 << 30) || p->Ny > (1 << 30) || p->Nz > (1 << 30))
     return set_error(POND_ERR_ARG, "grid out of range");
   const long long N = p->Nx * p->Ny * p->Nz;
   if (N > (1LL << 31) - 1) return set_error(POND_ERR_ARG, "grid has more than 2^31-1 nodes");
-  for (int k = 0; k < 3; k++)
-    if (p->bc[k] < POND_BC_PERIODIC || p->bc[k] > POND_BC_MIRROR) return set_error(POND_ERR_ARG, "bad bc[%d]", k);
-  if (!(p->tau > 0.5) || p->max_iter < 1 || !(p->tol_abs >= 0) || !(p->tol_rel >= 0))
-    return set_error(POND_ERR_ARG, "bad tau, max_iter or tolerance");
+  const int vst = check_step_params(p);
+  if (vst != POND_OK) return vst;
   const dim3 grd((unsigned)((p->Nx + d27::TX - 1) / d27::TX), (unsigned)((p->Ny + d27::TY - 1) / d27::TY),
                  (unsigned)((p->Nz + d27::TZ - 1) / d27::TZ));
   const long long nblocks = (long long)grd.x * grd.y * grd.z;
@@ -133,6 +152,8 @@ extern "C" int pond_step_noalloc(const pond_params* p, const float* f_in, const 
                      "(at most %d nodes, e.g. 256^3)",
                      (long long)p->Nx, (long long)p->Ny, (long long)p->Nz, nblocks, noalloc::kMaxBlocks,
                      noalloc::kMaxBlocks * d27::THREADS);
+  if (noalloc::any_overlap(N, f_in, rho_in, g_in, f_out, rho_out, g_out))
+    return set_error(POND_ERR_ARG, "pond_step_noalloc: an output buffer overlaps an input or another output");
   void* scratch = nullptr;
   int st = noalloc::setup_device(&scratch);
   if (st != POND_OK) return st;

@@ -17,6 +17,13 @@
 # Only comment markers and the template argument change; the binary name
 # carries the scheme unless it is lagr4.
 #
+# On D3Q125 the shipped calcStep launches PonDstepD3Q125 (update.cu:97) and
+# LBMpull takes its fixed-stencil D3Q125 block (steps.cu:366); both switches
+# are `#if defined D3Q125 && 1`.  For a D3Q125 scheme other than lagr4 the
+# two `&& 1` become `&& 0`, so the step runs PonDstep -> LBMpull's generic
+# branch with the selected interpolation call (the reference's own
+# alternative, as for the other lattices).
+#
 # bc = mirror sets the `outflow` flags of steps.cu.  On the D1Q5 / D3Q27
 # path only propagate<N>'s counts (steps.cu:1004-1013): the stencil is
 # reflected at every face with the populations reversed and u negated
@@ -36,7 +43,9 @@
 #   im2D.h           replaced by a stub: the GL/GLUT window code is not on
 #                    the step's path and no graphics stack exists here
 set -euo pipefail
-REF=${POND_REFERENCE_DIR:-/root/reference}
+# the reference's source tree: POND_REFERENCE_DIR, else a directory named
+# "reference" beside this repository
+REF=${POND_REFERENCE_DIR:-$(cd "$(dirname "$0")/../.." && pwd)/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/_ref"
 LAT=${1:?lattice}; PREC=${2:?precision}; NX=${3:?nx}; NY=${4:?ny}; NZ=${5:?nz}; SCHEME=${6:-lagr4}; BC=${7:-periodic}
@@ -86,6 +95,10 @@ case "$SCHEME" in
       grep -q '^#define NRMESH$' "$TMP/consts.h"
     fi ;;
 esac
+if [ "$LAT" = D3Q125 ] && [ "$SCHEME" != lagr4 ]; then
+  [ "$(grep -c '^  #if defined D3Q125 && 1$' "$TMP/steps.cu" "$TMP/update.cu" | awk -F: '{s+=$2} END {print s}')" -eq 2 ]
+  sed -i 's/^  #if defined D3Q125 \&\& 1$/  #if defined D3Q125 \&\& 0/' "$TMP/steps.cu" "$TMP/update.cu"
+fi
 cat > "$TMP/im2D.h" <<'EOF'
 #ifndef IM2D_H
 #define IM2D_H

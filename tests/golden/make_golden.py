@@ -138,6 +138,12 @@ def scheme_cases():
         bc="mirror")
     add("d3q125_mirror_8x4x4", 2, (8, 4, 4), 0.9, 2, smooth_state((8, 4, 4), 3, seed=32, modes=1, du=0.02), 32,
         "lagr4", bc="mirror")
+    # propagateWENO<3,5> on the 3D lattices (steps.cu:458; on D3Q125 through LBMpull's generic branch)
+    # (small velocities: the smoothness row of steps.cu:783 lies elsewhere in 3D, and with larger
+    # perturbations a few nodes of the float64 iteration cycle at the cap)
+    add("d3q27_weno5_8", 1, (8, 8, 8), 0.8, 2, smooth_state((8, 8, 8), 3, seed=33, modes=1, du=0.01), 33, "weno5")
+    add("d3q125_weno5_8x4x4", 2, (8, 4, 4), 0.9, 2, smooth_state((8, 4, 4), 3, seed=33, modes=1, du=0.01), 33,
+        "weno5")
     # the reference's TimeCorr after every step (halving dt: u / 2, T / 4)
     add("d1q5_timecorr_128", 0, (128, 1, 1), 0.8, 3, smooth_state((128, 1, 1), 1, seed=29, modes=2, T0=0.4), 29,
         "lagr4", timecorr=0.5)

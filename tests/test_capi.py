@@ -179,3 +179,59 @@ def test_mesh_calls_reject_null_context(pond):
     assert L.pond_amr_coarsen(None, 0.01, ctypes.byref(n)) == -1
     assert L.pond_rescale_time(None, 2.0) == -1
     assert L.pond_set_dt_adapt(None, 1, 1000, 4) == -1
+
+
+def _noalloc(L):
+    from lbmpond_b200 import _lib
+    fn = L.pond_step_noalloc
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.POINTER(_lib.PondParams)] + [ctypes.c_void_p] * 8
+    return fn
+
+
+@pytest.mark.parametrize("field,value,status,word", [
+    ("max_iter", 100001, -1, "max_iter"),   # bounds one launch on a shared GPU
+    ("tau", float("inf"), -1, "tau"),       # dtau would be 0
+    ("tol_abs", float("nan"), -1, "toleran"),
+    ("tol_rel", float("inf"), -1, "toleran"),
+    ("learned", 1, -5, "learned"),          # no predictor on this path
+    ("ddf", 1, -5, "energy"),
+])
+def test_noalloc_validates_before_device(pond, field, value, status, word):
+    """pond_step_noalloc applies pond_create's parameter checks and refuses
+    what it does not run, before any CUDA call (the pointers are never
+    dereferenced)."""
+    from lbmpond_b200 import _lib
+    L = _lib.load()
+    fn = _noalloc(L)
+    p = _lib.PondParams()
+    L.pond_params_default(1, ctypes.byref(p))
+    p.Nx, p.Ny, p.Nz = 32, 8, 4
+    setattr(p, field, value)
+    N = 32 * 8 * 4
+    bufs = [4096 + k * 4 * 32 * N for k in range(6)]  # disjoint fake addresses
+    assert fn(ctypes.byref(p), *bufs, 16, None) == status
+    assert word in L.pond_last_error_string().decode()
+
+
+@pytest.mark.parametrize("alias", ["f_out=f_in", "rho_out=g_in", "g_out inside f_in", "rho_out=g_out"])
+def test_noalloc_rejects_overlapping_buffers(pond, alias):
+    from lbmpond_b200 import _lib
+    L = _lib.load()
+    fn = _noalloc(L)
+    p = _lib.PondParams()
+    L.pond_params_default(1, ctypes.byref(p))
+    p.Nx, p.Ny, p.Nz = 32, 8, 4
+    N = 32 * 8 * 4
+    b = {k: 4096 + i * 4 * 32 * N for i, k in enumerate(("fi", "ri", "gi", "fo", "ro", "go"))}
+    if alias == "f_out=f_in":
+        b["fo"] = b["fi"]
+    elif alias == "rho_out=g_in":
+        b["ro"] = b["gi"] + 4 * N
+    elif alias == "g_out inside f_in":
+        b["go"] = b["fi"] + 4 * 26 * N
+    else:
+        b["ro"] = b["go"] + 4
+    st = fn(ctypes.byref(p), b["fi"], b["ri"], b["gi"], b["fo"], b["ro"], b["go"], 16, None)
+    assert st == -1
+    assert "overlaps" in L.pond_last_error_string().decode()

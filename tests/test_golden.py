@@ -94,14 +94,14 @@ def test_mesh_file_roundtrip(tmp_path):
     assert int(raw[0]) == 0x4D455348
 
 
-@pytest.mark.parametrize("idx", range(14))
+@pytest.mark.parametrize("idx", range(16))
 def test_scheme_cases_replay_cleanly(orc, idx):
     """Every alternative-scheme and mesh case converges everywhere in the oracle,
     so a fixture made from it by the reference's kernels compares node by node."""
     from tests.golden.make_golden import scheme_cases
     from tests.states import perturbed_populations
     cases = scheme_cases()
-    assert len(cases) == 14
+    assert len(cases) == 16
     c = cases[idx]
     rho, g = c["state"]
     t = orc.tables(c["lat"])

@@ -217,6 +217,30 @@ def test_init_and_errors(pond):
         assert s.diagnostics()["k"] > 0
 
 
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-9), ("fp32", 1e-4)])
+def test_tgv_kinetic_energy_matches_oracle(orc, pond, precision, tol):
+    """The TGV kinetic energy k of diagn.cu:3-22 (pond_diagnostics.k) against
+    the oracle's restatement, on the initial Taylor-Green state and after two
+    steps of each, in both precisions (float32 moves u by a few ulp, k by
+    twice that relative)."""
+    shape = (16, 16, 16)
+    with pond.Solver(lattice="D3Q27", shape=shape, interp=3, precision=precision, tau=0.51) as s:
+        s.init("tgv", 0.1, 1.0 / 12.0, 1.0, 5.0 / 3.0)
+        f, rho, g = s.get_state()
+        k0 = s.diagnostics()["k"]
+        s.step(2)
+        k2 = s.diagnostics()["k"]
+    st = orc.State(f, rho, g)
+    ref0 = orc.diagnostics(st, 1, shape)["k"]
+    assert k0 > 0 and abs(k0 - ref0) <= 1e-12 * ref0
+    for _ in range(2):
+        st, _, nc = orc.step(st, 1, shape, interp=3, tau=0.51)
+        assert nc == 0
+    ref2 = orc.diagnostics(st, 1, shape)["k"]
+    assert abs(k2 - ref2) <= tol * ref2, (k2, ref2)
+    assert k2 < k0  # viscous decay
+
+
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 @pytest.mark.parametrize("fault", ["nan_population", "nan_velocity", "negative_T"])
 @pytest.mark.parametrize("lat,shape,interp", [(1, (8, 8, 8), 4), (0, (64, 1, 1), 4), (2, (5, 4, 4), 6)])
