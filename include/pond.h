@@ -51,16 +51,25 @@ enum {
   POND_LAGR2 = 2, POND_LAGR3 = 3, POND_LAGR4 = 4, POND_LAGR5 = 5, /* propagate<N>, steps.cu:986 */
   POND_FIXED3 = 6, /* quadratic, origin fixed at coord-1: PonDstepD3Q125 steps.cu:151 */
   POND_TVD = 7,    /* flux-difference minmod form, steps.cu:118-124 with call site :447 */
-  POND_WENO5 = 8,  /* propagateWENO<3,5>, steps.cu:774-825 */
+  POND_WENO5 = 8,  /* propagateWENO<3,5>, steps.cu:774-825 (call site :458); in 3D the smoothness
+                      indicators read the row y = z = floor(crd.x+0.5) as the reference does (:783) */
   /* one-dimensional meshes (D1Q5, Ny = Nz = 1, periodic), with a node mask: */
   POND_GAP2 = 9,        /* linear between the nearest active nodes, propagate_nonequal_1D<2>,
                            steps.cu:1122-1149 (call site :449) */
-  POND_NONUNIFORM3 = 10 /* quadratic Lagrange on the node positions of x-1, x, x+1,
+  POND_NONUNIFORM3 = 10, /* quadratic Lagrange on the node positions of x-1, x, x+1,
                            propagateNR_1D + LagrPolNR_1D, steps.cu:882-908,590-594 (call site :453) */
+  /* WENO5 whose smoothness indicators read the row through the departure
+     point (y = floor(crd.y+0.5), z = floor(crd.z+0.5)) instead of the
+     reference's y = z = floor(crd.x+0.5); the same as POND_WENO5 on 1D grids */
+  POND_WENO5_ROW = 11
 };
 /* boundaries per axis: periodic is the reference (steps.cu:1015-1017); mirror
-   is its disabled outflow reflection (steps.cu:1004-1013); clamp = zero gradient */
-enum { POND_BC_PERIODIC = 0, POND_BC_CLAMP = 1, POND_BC_MIRROR = 2 };
+   is its disabled outflow reflection (steps.cu:1004-1013); clamp = zero gradient;
+   inflow = below the low end a ghost node at equilibrium in the state set by
+   pond_set_inflow (Dirichlet inflow), above the high end zero gradient
+   (outflow).  The reference has no inflow boundary.  Inflow runs with the
+   D3Q27/D3Q125 WENO5 schemes and the D3Q125 fixed-origin quadratic. */
+enum { POND_BC_PERIODIC = 0, POND_BC_CLAMP = 1, POND_BC_MIRROR = 2, POND_BC_INFLOW = 3 };
 /* arithmetic of populations, interpolation and collision; conserved-moment
    sums and the convergence test are float64 in both */
 enum { POND_FP32 = 0, POND_FP64 = 1 };
@@ -146,6 +155,11 @@ int pond_set_energy(pond_ctx* ctx, const double* h);
 int pond_get_energy(pond_ctx* ctx, double* h);
 /* any pointer may be NULL; each receives N values */
 int pond_get_fields(pond_ctx* ctx, double* rho, double* ux, double* uy, double* uz, double* T);
+/* state of the inflow ghost node of POND_BC_INFLOW axes: rho > 0, u, T > 0
+   (finite); needed before the first step of such a context.  Its populations
+   are f_i = rho w_i in the gauge (u, T) (set_base, lbpack.cu:15-21), with
+   energy populations at their equilibrium when the context carries them. */
+int pond_set_inflow(pond_ctx* ctx, double rho, double ux, double uy, double uz, double T);
 /* advance nsteps steps (calcStep without drop/diagnostics printing) */
 int pond_step(pond_ctx* ctx, int nsteps);
 int pond_diagnostics(pond_ctx* ctx, pond_diag* out);

@@ -22,16 +22,18 @@ import os
 import numpy as np
 
 from . import _lib
-from ._lib import (BC_CLAMP, BC_MIRROR, BC_PERIODIC, D1Q5, D3Q27, D3Q125, FIXED3, FP32, FP64, GAP2, IC_ACOUSTIC,
-                   IC_SOD_X, IC_SPHERE, IC_TGV, IC_UNIFORM, LAGR2, LAGR3, LAGR4, LAGR5, NONUNIFORM3, TVD, WENO5,
-                   PondError)
+from ._lib import (BC_CLAMP, BC_INFLOW, BC_MIRROR, BC_PERIODIC, D1Q5, D3Q27, D3Q125, FIXED3, FP32, FP64, GAP2,
+                   IC_ACOUSTIC, IC_SOD_X, IC_SPHERE, IC_TGV, IC_UNIFORM, LAGR2, LAGR3, LAGR4, LAGR5, NONUNIFORM3, TVD,
+                   WENO5, WENO5_ROW, PondError)
 
 __all__ = ["Solver", "PondError", "lattice_q", "lattice_tables", "D1Q5", "D3Q27", "D3Q125", "LAGR2", "LAGR3", "LAGR4", "LAGR5",
-           "FIXED3", "TVD", "WENO5", "GAP2", "NONUNIFORM3", "BC_PERIODIC", "BC_CLAMP", "BC_MIRROR", "FP32", "FP64",
+           "FIXED3", "TVD", "WENO5", "WENO5_ROW", "GAP2", "NONUNIFORM3", "BC_PERIODIC", "BC_CLAMP", "BC_MIRROR",
+           "BC_INFLOW", "FP32", "FP64",
            "IC_ACOUSTIC", "IC_SOD_X", "IC_SPHERE", "IC_TGV", "IC_UNIFORM", "write_arr", "read_arr"]
 
 _LATTICES = {"D1Q5": D1Q5, "D3Q27": D3Q27, "D3Q125": D3Q125}
-_BCS = {"periodic": BC_PERIODIC, "clamp": BC_CLAMP, "zero_gradient": BC_CLAMP, "mirror": BC_MIRROR}
+_BCS = {"periodic": BC_PERIODIC, "clamp": BC_CLAMP, "zero_gradient": BC_CLAMP, "mirror": BC_MIRROR,
+        "inflow": BC_INFLOW}
 _ICS = {"acoustic": IC_ACOUSTIC, "sod": IC_SOD_X, "sphere": IC_SPHERE, "tgv": IC_TGV, "uniform": IC_UNIFORM}
 
 
@@ -152,6 +154,10 @@ class Solver:
         out = [np.empty(self.N) for _ in range(5)]
         _lib.check(self._L.pond_get_fields(self._ctx, *[_dp(a) for a in out]))
         return dict(zip(("rho", "ux", "uy", "uz", "T"), out))
+
+    def set_inflow(self, rho, ux, uy, uz, T):
+        """State of the ghost node of ``"inflow"`` axes (equilibrium populations)."""
+        _lib.check(self._L.pond_set_inflow(self._ctx, float(rho), float(ux), float(uy), float(uz), float(T)))
 
     def step(self, n=1):
         _lib.check(self._L.pond_step(self._ctx, int(n)))

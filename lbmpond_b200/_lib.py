@@ -14,8 +14,8 @@ STATUS = {
 }
 
 D1Q5, D3Q27, D3Q125 = 0, 1, 2
-LAGR2, LAGR3, LAGR4, LAGR5, FIXED3, TVD, WENO5, GAP2, NONUNIFORM3 = 2, 3, 4, 5, 6, 7, 8, 9, 10
-BC_PERIODIC, BC_CLAMP, BC_MIRROR = 0, 1, 2
+LAGR2, LAGR3, LAGR4, LAGR5, FIXED3, TVD, WENO5, GAP2, NONUNIFORM3, WENO5_ROW = 2, 3, 4, 5, 6, 7, 8, 9, 10, 11
+BC_PERIODIC, BC_CLAMP, BC_MIRROR, BC_INFLOW = 0, 1, 2, 3
 FP32, FP64 = 0, 1
 IC_ACOUSTIC, IC_SOD_X, IC_SPHERE, IC_TGV, IC_UNIFORM = 0, 1, 2, 3, 4
 
@@ -65,6 +65,7 @@ SIGNATURES = {
     "pond_get_energy": (ctypes.c_int, [_vp, _dp]),
     "pond_get_fields": (ctypes.c_int, [_vp, _dp, _dp, _dp, _dp, _dp]),
     "pond_step": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "pond_set_inflow": (ctypes.c_int, [_vp] + [ctypes.c_double] * 5),
     "pond_diagnostics": (ctypes.c_int, [_vp, ctypes.POINTER(PondDiag)]),
     "pond_set_clock": (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.c_double, ctypes.c_double]),
     "pond_set_strict": (ctypes.c_int, [_vp, ctypes.c_int]),

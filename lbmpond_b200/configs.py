@@ -71,6 +71,12 @@ def shock_vortex_state(n, mach=1.5, T1=0.1, eps=0.3, radius=0.05, gamma=5.0 / 3.
     return flat(rho), np.stack([flat(ux), flat(uy), np.zeros(n ** 3), flat(T)])
 
 
+def shock_vortex_inflow(mach=1.5, T1=0.1, gamma=5.0 / 3.0):
+    """The pre-shock state (rho, u_x, u_y, u_z, T) the inflow boundary holds
+    below x = 0: the upstream side of shock_vortex_state."""
+    return (1.0, mach * np.sqrt(gamma * T1), 0.0, 0.0, T1)
+
+
 def tgv_params(gamma: float = 5.0 / 3.0, mach: float = 0.5):
     """Compressible Taylor-Green vortex (pond_init POND_IC_TGV): U0, T0, rho0,
     gamma with T0 = TLat/4 of D3Q27 and U0 = mach * sqrt(gamma T0)."""
@@ -96,6 +102,7 @@ def _shock_vortex_init(gamma):
     def init(s, n):
         rho, g = shock_vortex_state(n, gamma=gamma)
         s.set_state(rho, g)
+        s.set_inflow(*shock_vortex_inflow(gamma=gamma))
     return init
 
 
@@ -125,13 +132,19 @@ PRESETS = {
         lambda s, n: s.init("sphere", *sphere_params()), 1500),
     "shock_vortex_d3q125": Preset(
         "D3Q125 Mach 1.5 normal shock at x = 0.5 + isentropic vortex (strength 0.3, radius 0.05) at (0.25, 0.5), "
-        "fixed-origin quadratic, tau 0.9, zero-gradient x ends, periodic y and z, float32",
+        "WENO5 (smoothness row through the departure point), tau 0.9, inflow of the pre-shock state below x = 0 "
+        "and zero-gradient outflow above x = 1, periodic y and z, float32",
+        192, lambda n: dict(lattice="D3Q125", shape=(n, n, n), precision="fp32", tau=0.9, interp=11,
+                            bc=("inflow", "periodic", "periodic")), _shock_vortex_init(5.0 / 3.0), 1000),
+    "shock_vortex_d3q125_fixed3": Preset(
+        "the shock and vortex with the reference's D3Q125 scheme (fixed-origin quadratic, steps.cu:151-250)",
         192, lambda n: dict(lattice="D3Q125", shape=(n, n, n), precision="fp32", tau=0.9,
-                            bc=("clamp", "periodic", "periodic")), _shock_vortex_init(5.0 / 3.0), 1000),
+                            bc=("inflow", "periodic", "periodic")), _shock_vortex_init(5.0 / 3.0), 1000),
     "shock_vortex_d3q125_gamma14": Preset(
-        "the shock and vortex as a gamma = 1.4 gas (energy populations, 2 extra degrees of freedom)",
+        "the shock and vortex as a gamma = 1.4 gas (energy populations, 2 extra degrees of freedom; "
+        "fixed-origin quadratic)",
         192, lambda n: dict(lattice="D3Q125", shape=(n, n, n), precision="fp32", tau=0.9,
-                            bc=("clamp", "periodic", "periodic"), ddf_dof=2), _shock_vortex_init(1.4), 1000),
+                            bc=("inflow", "periodic", "periodic"), ddf_dof=2), _shock_vortex_init(1.4), 1000),
 }
 
 

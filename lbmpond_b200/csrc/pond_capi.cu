@@ -80,7 +80,7 @@ double lattice_dim(int lattice) { return lattice == POND_D1Q5 ? 1.0 : 3.0; }
 // length of one step launch on a shared GPU.
 int check_step_params(const pond_params* p) {
   for (int a = 0; a < 3; a++)
-    if (p->bc[a] < POND_BC_PERIODIC || p->bc[a] > POND_BC_MIRROR) return set_error(POND_ERR_ARG, "bad bc[%d]", a);
+    if (p->bc[a] < POND_BC_PERIODIC || p->bc[a] > POND_BC_INFLOW) return set_error(POND_ERR_ARG, "bad bc[%d]", a);
   if (!(p->tau > 0.5) || !std::isfinite(p->tau)) return set_error(POND_ERR_ARG, "tau must be a finite value > 0.5");
   if (p->max_iter < 1 || p->max_iter > 100000) return set_error(POND_ERR_ARG, "max_iter out of range (1..100000)");
   if (!(p->tol_abs >= 0) || !(p->tol_rel >= 0) || !std::isfinite(p->tol_abs) || !std::isfinite(p->tol_rel))
@@ -92,9 +92,10 @@ bool scheme_supported(int lattice, int interp) {
   switch (lattice) {
     case POND_D1Q5:
       return (interp >= POND_LAGR2 && interp <= POND_LAGR5) || interp == POND_TVD || interp == POND_WENO5 ||
-             interp == POND_GAP2 || interp == POND_NONUNIFORM3;
-    case POND_D3Q27: return interp >= POND_LAGR2 && interp <= POND_LAGR5;
-    case POND_D3Q125: return interp == POND_FIXED3;
+             interp == POND_WENO5_ROW || interp == POND_GAP2 || interp == POND_NONUNIFORM3;
+    case POND_D3Q27: return (interp >= POND_LAGR2 && interp <= POND_LAGR5) || interp == POND_WENO5 ||
+                            interp == POND_WENO5_ROW;
+    case POND_D3Q125: return interp == POND_FIXED3 || interp == POND_WENO5 || interp == POND_WENO5_ROW;
     default: return false;
   }
 }
@@ -260,7 +261,18 @@ int pond_create(const pond_params* p, pond_ctx** out) {
     return set_error(POND_ERR_UNSUPPORTED, "interpolation %d is not available for lattice %d", p->interp, p->lattice);
   const int vst = check_step_params(p);
   if (vst != POND_OK) return vst;
-  if (p->lattice == POND_D1Q5 && (p->interp == POND_TVD || p->interp == POND_WENO5) && (p->Ny != 1 || p->Nz != 1))
+  {
+    bool inflow = false;
+    for (int a = 0; a < 3; a++) inflow = inflow || p->bc[a] == POND_BC_INFLOW;
+    const bool weno3d = p->lattice != POND_D1Q5 && (p->interp == POND_WENO5 || p->interp == POND_WENO5_ROW);
+    if (inflow && !weno3d && !(p->lattice == POND_D3Q125 && p->interp == POND_FIXED3))
+      return set_error(POND_ERR_UNSUPPORTED,
+                       "the inflow boundary runs with the D3Q27/D3Q125 WENO5 schemes and the D3Q125 fixed-origin quadratic");
+    if (weno3d && p->ddf)
+      return set_error(POND_ERR_UNSUPPORTED, "WENO5 on the 3D lattices carries no energy populations");
+  }
+  if (p->lattice == POND_D1Q5 && (p->interp == POND_TVD || p->interp == POND_WENO5 || p->interp == POND_WENO5_ROW) &&
+      (p->Ny != 1 || p->Nz != 1))
     return set_error(POND_ERR_UNSUPPORTED, "TVD/WENO5 run on 1D grids (Ny = Nz = 1)");
   if (p->lattice == POND_D1Q5 && mesh_scheme(p->interp)) {
     if (p->Ny != 1 || p->Nz != 1 || p->Nx < 3) return set_error(POND_ERR_UNSUPPORTED, "mesh schemes run on 1D grids, Nx >= 3");
@@ -510,6 +522,17 @@ int pond_get_niter(pond_ctx* c, int32_t* out) {
   cudaError_t e = cudaMemcpyAsync(out, c->niter, sizeof(int) * c->N, cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_fail(e, "pond_get_niter");
+  return POND_OK;
+}
+
+int pond_set_inflow(pond_ctx* c, double rho, double ux, double uy, double uz, double T) {
+  if (!c) return set_error(POND_ERR_ARG, "null argument");
+  if (!(rho > 0) || !(T > 0) || !std::isfinite(rho) || !std::isfinite(T) || !std::isfinite(ux) ||
+      !std::isfinite(uy) || !std::isfinite(uz))
+    return set_error(POND_ERR_ARG, "inflow state needs finite rho > 0, u and T > 0");
+  const double v[5] = {rho, ux, uy, uz, T};
+  for (int k = 0; k < 5; k++) c->inflow[k] = v[k];
+  c->have_inflow = true;
   return POND_OK;
 }
 

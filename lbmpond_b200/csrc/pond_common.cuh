@@ -187,6 +187,8 @@ template <typename R> struct StepArgs {
   // each in node order (thread t of the mesh kernels takes node part[t]), or null
   const int* part = nullptr;      // [N]
   long long n_active = 0;
+  // state of the inflow ghost node of POND_BC_INFLOW axes: rho, u_x, u_y, u_z, T
+  double inflow[5] = {1, 0, 0, 0, 1};
 };
 
 }  // namespace pond

@@ -58,6 +58,9 @@ struct pond_ctx {
   unsigned long long* amr_counts = nullptr;  // [4] device counters
   unsigned long long* amr_counts_h = nullptr;  // pinned copy
   bool strict = false;  // pond_step stops with POND_ERR_NOT_CONVERGED after a step with nodes at max_iter
+  // ghost state of POND_BC_INFLOW axes (pond_set_inflow): rho, u_x, u_y, u_z, T
+  double inflow[5] = {1, 0, 0, 0, 1};
+  bool have_inflow = false;
   // time-step adaptation after every step (update.cu:121-123)
   bool dt_adapt = false;
   int adapt_hi = 1000, adapt_lo = 4;

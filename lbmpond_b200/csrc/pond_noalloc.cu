@@ -143,6 +143,8 @@ extern "C" int pond_step_noalloc(const pond_params* p, const float* f_in, const 
   if (N > (1LL << 31) - 1) return set_error(POND_ERR_ARG, "grid has more than 2^31-1 nodes");
   const int vst = check_step_params(p);
   if (vst != POND_OK) return vst;
+  for (int k = 0; k < 3; k++)
+    if (p->bc[k] == POND_BC_INFLOW) return set_error(POND_ERR_UNSUPPORTED, "pond_step_noalloc has no inflow boundary");
   const dim3 grd((unsigned)((p->Nx + d27::TX - 1) / d27::TX), (unsigned)((p->Ny + d27::TY - 1) / d27::TY),
                  (unsigned)((p->Nz + d27::TZ - 1) / d27::TZ));
   const long long nblocks = (long long)grd.x * grd.y * grd.z;

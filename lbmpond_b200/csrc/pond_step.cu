@@ -13,6 +13,7 @@
 #include "pond_step_d3q125_tile.cuh"
 #include "pond_step_d3q27.cuh"
 #include "pond_step_point.cuh"
+#include "pond_step_weno3d.cuh"
 
 namespace pond {
 
@@ -204,6 +205,10 @@ template <typename R> static int launch_typed(pond_ctx* c, const void* const* in
   a.kdx = kdx_of(c);
   a.mask = c->mask[0] ? c->mask[c->mask_cur] : nullptr;
   a.pos = c->pos;
+  for (int k = 0; k < 3; k++)
+    if (c->p.bc[k] == POND_BC_INFLOW && !c->have_inflow)
+      return set_error(POND_ERR_STATE, "an inflow boundary needs pond_set_inflow before stepping");
+  for (int k = 0; k < 5; k++) a.inflow[k] = c->inflow[k];
   if (c->mask[0]) {
     const int pst = mesh_partition(c);
     if (pst != POND_OK) return pst;
@@ -251,8 +256,25 @@ template <typename R> static int launch_typed(pond_ctx* c, const void* const* in
       case POND_LAGR4: pull_1d_energy_kernel<POND_LAGR4, R><<<g1, 128, 0, s>>>(a); break;
       case POND_LAGR5: pull_1d_energy_kernel<POND_LAGR5, R><<<g1, 128, 0, s>>>(a); break;
       case POND_TVD: pull_1d_energy_kernel<POND_TVD, R><<<g1, 128, 0, s>>>(a); break;
-      case POND_WENO5: pull_1d_energy_kernel<POND_WENO5, R><<<g1, 128, 0, s>>>(a); break;
+      case POND_WENO5:
+      case POND_WENO5_ROW: pull_1d_energy_kernel<POND_WENO5, R><<<g1, 128, 0, s>>>(a); break;
       default: return set_error(POND_ERR_UNSUPPORTED, "scheme");
+    }
+    e = cudaGetLastError();
+    return e == cudaSuccess ? POND_OK : cuda_fail(e, "step kernel launch");
+  }
+  if (c->p.lattice != POND_D1Q5 && (c->p.interp == POND_WENO5 || c->p.interp == POND_WENO5_ROW)) {
+    const bool fix = c->p.interp == POND_WENO5_ROW;
+    if (c->p.lattice == POND_D3Q27) {
+      const long long per = (long long)w3d::WARPS * w3d::Geo<POND_D3Q27>::NPW;
+      const unsigned grd = (unsigned)((a.N + per - 1) / per);
+      if (fix) w3d::pull_weno3d_kernel<POND_D3Q27, R, true><<<grd, w3d::THREADS, 0, s>>>(a);
+      else w3d::pull_weno3d_kernel<POND_D3Q27, R, false><<<grd, w3d::THREADS, 0, s>>>(a);
+    } else {
+      const long long per = (long long)w3d::WARPS * w3d::Geo<POND_D3Q125>::NPW;
+      const unsigned grd = (unsigned)((a.N + per - 1) / per);
+      if (fix) w3d::pull_weno3d_kernel<POND_D3Q125, R, true><<<grd, w3d::THREADS, 0, s>>>(a);
+      else w3d::pull_weno3d_kernel<POND_D3Q125, R, false><<<grd, w3d::THREADS, 0, s>>>(a);
     }
     e = cudaGetLastError();
     return e == cudaSuccess ? POND_OK : cuda_fail(e, "step kernel launch");
@@ -268,6 +290,7 @@ template <typename R> static int launch_typed(pond_ctx* c, const void* const* in
           pull_1d_scheme_kernel<POND_TVD, R><<<(a.nx + 127) / 128, 128, 0, s>>>(a);
           break;
         case POND_WENO5:
+        case POND_WENO5_ROW:  // one row on a 1D grid: both read row 0
           pull_1d_scheme_kernel<POND_WENO5, R><<<(a.nx + 127) / 128, 128, 0, s>>>(a);
           break;
         case POND_GAP2:

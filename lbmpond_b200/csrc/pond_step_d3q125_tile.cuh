@@ -58,13 +58,26 @@ static_assert(2 * (sizeof(SmemT<false>) + 1024) <= 233472, "two CTAs must fit in
 static_assert(sizeof(SmemT<true>) + 1024 <= 233472, "the energy variant must fit one CTA per SM");
 static_assert(sizeof(SmemT<false, double>) <= 232448, "the float64 tile must fit one CTA");
 
-// global node of staged node i and its mirror flags
+// one axis of a staged position: the index, with the inflow boundary's
+// ghost below the low end (*ghost) and zero gradient above the high end
+__device__ __forceinline__ int staged_axis(int p, int n, int bc, bool& rev, bool& ghost) {
+  if (bc == POND_BC_INFLOW) {
+    rev = false;
+    if (p < 0) { ghost = true; return 0; }
+    return p >= n ? n - 1 : p;
+  }
+  return resolve_axis(p, n, bc, rev);
+}
+
+// global node of staged node i and its mirror flags; -1 for the inflow ghost
 template <typename Rs>
 __device__ __forceinline__ int staged_global(const StepArgs<Rs>& a, int x0, int y0, int z0, int i, bool rv[3]) {
   const int hx = i % S, hy = (i / S) % S, hz = i / (S * S);
-  const int gx = resolve_axis(x0 - 1 + hx, a.nx, a.bc[0], rv[0]);
-  const int gy = resolve_axis(y0 - 1 + hy, a.ny, a.bc[1], rv[1]);
-  const int gz = resolve_axis(z0 - 1 + hz, a.nz, a.bc[2], rv[2]);
+  bool ghost = false;
+  const int gx = staged_axis(x0 - 1 + hx, a.nx, a.bc[0], rv[0], ghost);
+  const int gy = staged_axis(y0 - 1 + hy, a.ny, a.bc[1], rv[1], ghost);
+  const int gz = staged_axis(z0 - 1 + hz, a.nz, a.bc[2], rv[2], ghost);
+  if (ghost) { rv[0] = rv[1] = rv[2] = false; return -1; }
   return gx + a.nx * (gy + a.ny * gz);
 }
 
@@ -119,16 +132,27 @@ __global__ void __launch_bounds__(THREADS, (kE || sizeof(R) == 8) ? 1 : 2) pull_
     sm.flags[i] = (unsigned char)((rv[0] ? 1 : 0) | (rv[1] ? 2 : 0) | (rv[2] ? 4 : 0));
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-      const R v = a.g_in[(long long)k * a.N + g];
+      const R v = g < 0 ? R(a.inflow[1 + k]) : a.g_in[(long long)k * a.N + g];
       sm.u[k][i] = rv[k] ? -v : v;
     }
-    const R Tn = a.g_in[3 * a.N + g];
+    const R Tn = g < 0 ? R(a.inflow[4]) : a.g_in[3 * a.N + g];
     sm.c[i] = copysign(sqrt(fabs(Tn) * R(1.0 / L::TLat)), Tn);
   }
   for (int idx = tid; idx < 125 * SN; idx += THREADS) {
     const int p = idx / SN, i = idx - p * SN;
     bool rv[3];
     const int g = staged_global(a, x0, y0, z0, i, rv);
+    if (g < 0) {  // the inflow ghost: set_base of the inflow state (and its energy equilibrium)
+      const double w = lattice_weight_t<POND_D3Q125>(p);
+      sm.f[p * PS + i] = R(a.inflow[0] * w);
+      if constexpr (kE) {
+        const double C = sqrt(a.inflow[4] / L::TLat);
+        const double vx = C * xi5(p / 25) + a.inflow[1], vy = C * xi5((p / 5) % 5) + a.inflow[2],
+                     vz = C * xi5(p % 5) + a.inflow[3];
+        sm.h[p * PS + i] = R(a.inflow[0] * w * (vx * vx + vy * vy + vz * vz + a.dof * a.inflow[4]));
+      }
+      continue;
+    }
     const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(&sm.f[p * PS + i]));
     if constexpr (sizeof(R) == 8)
       asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(a.f_in + (long long)p * a.N + g)

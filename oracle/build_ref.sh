@@ -60,6 +60,7 @@ case "$PREC" in double|float) ;; *) echo "bad precision $PREC" >&2; exit 2;; esa
 if (( NX % 4 != 0 )); then echo "nx must be a multiple of 4 (brick.x)" >&2; exit 2; fi
 if [ ! -f "$REF/steps.cu" ]; then echo "reference sources not found at $REF" >&2; exit 3; fi
 NVCC=${NVCC:-nvcc}
+EXTRA=()
 mkdir -p "$OUT"
 BIN="$OUT/ref_pond_${LAT}_${PREC}_${NX}x${NY}x${NZ}"
 if [ "$SCHEME" != lagr4 ]; then BIN="${BIN}_${SCHEME}"; fi
@@ -98,6 +99,7 @@ esac
 if [ "$LAT" = D3Q125 ] && [ "$SCHEME" != lagr4 ]; then
   [ "$(grep -c '^  #if defined D3Q125 && 1$' "$TMP/steps.cu" "$TMP/update.cu" | awk -F: '{s+=$2} END {print s}')" -eq 2 ]
   sed -i 's/^  #if defined D3Q125 \&\& 1$/  #if defined D3Q125 \&\& 0/' "$TMP/steps.cu" "$TMP/update.cu"
+  EXTRA=(-DPOND_REF_D3Q125_PULL)  # oracle/ref_main.cu mirrors calcStep's launch switch
 fi
 cat > "$TMP/im2D.h" <<'EOF'
 #ifndef IM2D_H
@@ -109,6 +111,6 @@ FLAGS=(-gencode arch=compute_100a,code=sm_100a -O3 -rdc=true -I"$TMP" -Xcudafe -
 for f in update init lbpack diagn drop; do
   "$NVCC" "${FLAGS[@]}" -c "$TMP/$f.cu" -o "$TMP/$f.o"
 done
-"$NVCC" "${FLAGS[@]}" -c "$HERE/ref_main.cu" -o "$TMP/ref_main.o"
+"$NVCC" "${FLAGS[@]}" "${EXTRA[@]}" -c "$HERE/ref_main.cu" -o "$TMP/ref_main.o"
 "$NVCC" -gencode arch=compute_100a,code=sm_100a -rdc=true "$TMP"/*.o -o "$BIN"
 echo "$BIN"

@@ -22,8 +22,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liborc.so")
 
 D1Q5, D3Q27, D3Q125 = 0, 1, 2
-LAGR2, LAGR3, LAGR4, LAGR5, FIXED3, TVD, WENO5, GAP2, NONUNIFORM3 = 2, 3, 4, 5, 6, 7, 8, 9, 10
-BC_PERIODIC, BC_CLAMP, BC_MIRROR = 0, 1, 2
+LAGR2, LAGR3, LAGR4, LAGR5, FIXED3, TVD, WENO5, GAP2, NONUNIFORM3, WENO5_ROW = 2, 3, 4, 5, 6, 7, 8, 9, 10, 11
+BC_PERIODIC, BC_CLAMP, BC_MIRROR, BC_INFLOW = 0, 1, 2, 3
 
 # reference defaults: steps.cu:451 propagate<4> for D1Q5/D3Q27, and the
 # fixed-origin quadratic D3Q125 kernel (steps.cu:151, launched update.cu:98)
@@ -44,6 +44,7 @@ class _Params(ctypes.Structure):
         ("max_iter", ctypes.c_int),
         ("nthreads", ctypes.c_int),
         ("dof", ctypes.c_double),
+        ("inflow", ctypes.c_double * 5),
     ]
 
 
@@ -198,10 +199,11 @@ def base_state(lattice: int, rho, ux, uy, uz, T) -> State:
 
 
 def step(state: State, lattice: int, shape, interp=None, tau=0.9, tol_abs=1e-12, tol_rel=1e-10,
-         max_iter=100, bc=(BC_PERIODIC,) * 3, guess=None, nthreads=0, dof=None):
+         max_iter=100, bc=(BC_PERIODIC,) * 3, guess=None, nthreads=0, dof=None, inflow=None):
     """One pull step; returns (new_state, niter[N], nonconverged_count).  A
     state with energy populations (``state.h``) steps with the
-    double-distribution extension and needs ``dof``."""
+    double-distribution extension and needs ``dof``.  ``inflow`` = (rho,
+    u_x, u_y, u_z, T) of the ghost node of BC_INFLOW axes."""
     L = lib()
     nx, ny, nz = shape
     N = nx * ny * nz
@@ -212,7 +214,8 @@ def step(state: State, lattice: int, shape, interp=None, tau=0.9, tol_abs=1e-12,
     if ddf and dof is None:
         raise ValueError("a state with energy populations needs dof")
     p = _Params(lattice, interp, nx, ny, nz, (ctypes.c_int * 3)(*bc), tau, tol_abs, tol_rel,
-                max_iter, nthreads, float(dof) if ddf else 0.0)
+                max_iter, nthreads, float(dof) if ddf else 0.0,
+                (ctypes.c_double * 5)(*(inflow if inflow is not None else (1.0, 0.0, 0.0, 0.0, 1.0))))
     f_in = np.ascontiguousarray(state.f, dtype=np.float64)
     r_in = np.ascontiguousarray(state.rho, dtype=np.float64)
     g_in = np.ascontiguousarray(state.g, dtype=np.float64)

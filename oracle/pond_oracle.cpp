@@ -329,6 +329,8 @@ struct Domain {
   int bc[3];
   const uint8_t* mask = nullptr;  // Cinfo::set per node (nullptr: every node active)
   const double* pos = nullptr;    // Cell::p.x per node under NRMESH (nullptr: p_x = x)
+  double inflow[5] = {1, 0, 0, 0, 1};  // ghost state of ORC_BC_INFLOW axes: rho, u, T
+  double dof = 0;                      // energy populations of the ghost (double-distribution extension)
 };
 
 inline int64_t wrapi(int64_t p, int64_t n) { return ((p % n) + n) % n; }
@@ -342,7 +344,14 @@ void load_cell(const Domain& D, int64_t px, int64_t py, int64_t pz, Cell& c) {
   bool rev[3] = {false, false, false};
   for (int a = 0; a < 3; a++) {
     const int64_t n = D.n[a];
-    if (D.bc[a] == ORC_BC_MIRROR) {
+    if (D.bc[a] == ORC_BC_INFLOW && p[a] < 0) {  // the inflow ghost: set_base of the inflow state
+      set_base(*D.L, c, D.inflow[0], D.inflow + 1);
+      if (D.h) set_energy(*D.L, c, D.dof);
+      return;
+    }
+    if (D.bc[a] == ORC_BC_INFLOW) {  // outflow end: zero gradient
+      if (p[a] >= n) p[a] = n - 1;
+    } else if (D.bc[a] == ORC_BC_MIRROR) {
       if (p[a] < 0) { p[a] = -1 - p[a]; rev[a] = true; }
       if (p[a] >= n) { p[a] = n - 1 - p[a] + n; rev[a] = true; }
       p[a] = wrapi(p[a], n);
@@ -416,8 +425,13 @@ double lagr_eval(const Domain& D, int N, const double crd[3], const int64_t cl[3
   return fpr;
 }
 
-// steps.cu:774-825 propagateWENO<3,5>
-double propagate_weno5(const Domain& D, const double crd[3], int i, const double* base, bool energy = false) {
+// steps.cu:774-825 propagateWENO<3,5>.  row_fix: the smoothness indicators
+// read the row through the departure point (y = floor(crd.y+0.5), z =
+// floor(crd.z+0.5), the first row of the three sub-stencils) instead of the
+// reference's y = z = floor(crd.x+0.5) (:783), which in 3D lies elsewhere in
+// the domain; on 1D grids both are row 0.
+double propagate_weno5(const Domain& D, const double crd[3], int i, const double* base, bool energy = false,
+                       bool row_fix = false) {
   const double fx = std::floor(crd[0] + 0.5), fy = std::floor(crd[1] + 0.5), fz = std::floor(crd[2] + 0.5);
   const int64_t c0[3] = {(int64_t)(fx - 2), (int64_t)fy, (int64_t)fz};
   const int64_t c1[3] = {(int64_t)(fx - 1), (int64_t)fy, (int64_t)fz};
@@ -430,7 +444,7 @@ double propagate_weno5(const Domain& D, const double crd[3], int i, const double
   const double d2 = (cdist * cdist + 3 * cdist + 2) / 12.;
   const double d1 = 1. - d0 - d2;
   // :783 -- the smoothness row uses y = z = floor(crd.x+0.5) (wrapped)
-  const int64_t lx = (int64_t)(fx - 2), ly = (int64_t)fx, lz = (int64_t)fx;
+  const int64_t lx = (int64_t)(fx - 2), ly = (int64_t)(row_fix ? fy : fx), lz = (int64_t)(row_fix ? fz : fx);
   double u[6];
   Cell c;
   for (int k = 1; k <= 5; k++) {
@@ -603,9 +617,12 @@ int pull_node(const Domain& D, const orc_params& P, int64_t x, int64_t y, int64_
           if (ddf) cnew.h[i] = propagate_tvd(D, coord, vi[i], i, uT, true);
           break;
         case ORC_WENO5:
-          val = propagate_weno5(D, crd, i, uT);
-          if (ddf) cnew.h[i] = propagate_weno5(D, crd, i, uT, true);
+        case ORC_WENO5_ROW: {
+          const bool fix = P.interp == ORC_WENO5_ROW;
+          val = propagate_weno5(D, crd, i, uT, false, fix);
+          if (ddf) cnew.h[i] = propagate_weno5(D, crd, i, uT, true, fix);
           break;
+        }
         case ORC_GAP2:  // call site steps.cu:449
           val = propagate_gap2(D, crd, i, uT);
           break;
@@ -736,6 +753,8 @@ int64_t orc_step_ddf(const orc_params* p, const double* f_in, const double* h_in
   D.n[0] = p->nx; D.n[1] = p->ny; D.n[2] = p->nz;
   D.N = p->nx * p->ny * p->nz;
   for (int a = 0; a < 3; a++) D.bc[a] = p->bc[a];
+  for (int k = 0; k < 5; k++) D.inflow[k] = p->inflow[k];
+  D.dof = p->dof;
   const orc_params P = *p;
   int64_t nonconv = 0;
   const int64_t N = D.N;

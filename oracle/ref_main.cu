@@ -28,6 +28,10 @@
 // mask and positions.  Mesh file: uint32 magic 0x4d455348, int64 N, uint8
 // mask[N], float64 pos[N].
 //
+// A D3Q125 build with -DPOND_REF_D3Q125_PULL launches PonDstep (LBMpull)
+// instead of PonDstepD3Q125, as the reference's calcStep does once its
+// `#if defined D3Q125 && 1` (update.cu:97) reads `&& 0`.
+//
 // With POND_REF_TIMECORR=s in the environment the driver also runs the
 // reference's TimeCorr(s) (update.cu:15-28: u *= s, T *= s*s, its call
 // commented at update.cu:123) after every step, before the swap, and scales
@@ -211,9 +215,9 @@ int main(int argc, char** argv) {
     CHECK_ERROR(cudaMemset(parsHost.moment, 0, sizeof(ftype3)));
     CHECK_ERROR(cudaEventRecord(t0));
     const dim3 block(parsHost.Nx / brick.x, parsHost.Ny / brick.y, parsHost.Nz / brick.z);
-#if defined D3Q125
+#if defined D3Q125 && !defined POND_REF_D3Q125_PULL
     PonDstepD3Q125<<<dim3(parsHost.Nx, parsHost.Ny, parsHost.Nz), Qn>>>();
-#else
+#else  // (with POND_REF_D3Q125_PULL a D3Q125 build takes calcStep's other branch, update.cu:99)
     PonDstep<<<block, brick>>>();
 #endif
     CHECK_ERROR(cudaEventRecord(t1));

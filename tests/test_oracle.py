@@ -170,3 +170,53 @@ def test_guess_changes_only_start(orc):
     assert np.allclose(out2.g, out.g, rtol=1e-9, atol=1e-11)
     assert np.allclose(out2.f, out.f, rtol=1e-9, atol=1e-11)
     assert n1.mean() <= n0.mean()
+
+
+def test_weno5_row_equals_weno5_on_1d_grids(orc):
+    """On a 1D grid the reference's smoothness row (y = z = floor(crd.x+0.5),
+    wrapped) and the row through the departure point are both row 0."""
+    from tests.states import perturbed_populations, smooth_state
+    shape = (64, 1, 1)
+    rho, g = smooth_state(shape, 1, seed=5, modes=2)
+    st = orc.State(perturbed_populations(orc, 0, rho, g, seed=5), rho, g)
+    a, na, _ = orc.step(st, 0, shape, interp=orc.WENO5, tau=0.7)
+    b, nb, _ = orc.step(st, 0, shape, interp=orc.WENO5_ROW, tau=0.7)
+    assert np.array_equal(a.f, b.f) and np.array_equal(a.g, b.g) and np.array_equal(na, nb)
+
+
+@pytest.mark.parametrize("lat,interp", [(2, 6), (2, 11), (1, 8)])
+def test_inflow_ghost_equals_clamp_on_an_equilibrium_face(orc, lat, interp):
+    """The inflow ghost holds set_base(rho, u, T) of the inflow state; when the
+    x = 0 face is uniform, at equilibrium and in that state, one step with
+    inflow/outflow in x equals one step with zero gradient at both x ends."""
+    from tests.states import smooth_state
+    shape = (7, 4, 3)
+    rho, g = smooth_state(shape, 3, seed=8, modes=1, du=0.01)
+    face = np.arange(rho.size) % shape[0] == 0
+    state0 = (1.05, 0.1, -0.02, 0.01, 0.11)
+    rho[face] = state0[0]
+    for k in range(4):
+        g[k][face] = state0[1 + k]
+    t = orc.tables(lat)
+    f = t.w[:, None] * rho[None, :]
+    st = orc.State(f, rho, g)
+    a, na, nca = orc.step(st, lat, shape, interp=interp, tau=0.8, bc=(3, 0, 0), inflow=state0)
+    b, nb, ncb = orc.step(st, lat, shape, interp=interp, tau=0.8, bc=(1, 0, 0))
+    assert nca == 0 and ncb == 0
+    assert np.array_equal(a.f, b.f) and np.array_equal(a.g, b.g)
+
+
+@pytest.mark.parametrize("lat,interp,T0", [(2, 6, 0.1), (2, 11, 0.1), (1, 11, 0.25)])
+def test_uniform_inflow_flow_is_a_fixed_point(orc, lat, interp, T0):
+    shape = (8, 3, 3)
+    N = int(np.prod(shape))
+    state0 = (1.0, 0.3, 0.0, 0.0, T0)
+    g = np.zeros((4, N)); g[0] = state0[1]; g[3] = T0
+    rho = np.full(N, 1.0)
+    t = orc.tables(lat)
+    st = orc.State(t.w[:, None] * rho[None, :], rho, g)
+    for _ in range(2):
+        st, niter, nc = orc.step(st, lat, shape, interp=interp, tau=0.9, bc=(3, 0, 0), inflow=state0)
+        assert nc == 0
+    assert np.abs(st.rho - 1).max() < 1e-13 and np.abs(st.g[0] - 0.3).max() < 1e-13
+    assert np.abs(st.g[3] - T0).max() < 1e-13
