@@ -46,7 +46,10 @@ def sphere_state(n: int, lam: float = SPHERE_LAMBDA):
     return rho, np.stack([zero, zero, zero, T])
 
 
-def shock_vortex_state(n, mach=1.5, T1=0.1, eps=0.3, radius=0.05, gamma=5.0 / 3.0):
+SHOCK_T1 = 0.05  # pre-shock lattice temperature: every |v| stays below 1.1 nodes per step (TLat = 1)
+
+
+def shock_vortex_state(n, mach=1.5, T1=SHOCK_T1, eps=0.3, radius=0.05, gamma=5.0 / 3.0):
     """Stationary normal shock at x = 0.5 (pre-shock rho = 1, T = T1, flow
     along +x at `mach`; post-shock state from the Rankine-Hugoniot
     relations) and an isentropic vortex of strength `eps` (velocity scale
@@ -71,7 +74,7 @@ def shock_vortex_state(n, mach=1.5, T1=0.1, eps=0.3, radius=0.05, gamma=5.0 / 3.
     return flat(rho), np.stack([flat(ux), flat(uy), np.zeros(n ** 3), flat(T)])
 
 
-def shock_vortex_inflow(mach=1.5, T1=0.1, gamma=5.0 / 3.0):
+def shock_vortex_inflow(mach=1.5, T1=SHOCK_T1, gamma=5.0 / 3.0):
     """The pre-shock state (rho, u_x, u_y, u_z, T) the inflow boundary holds
     below x = 0: the upstream side of shock_vortex_state."""
     return (1.0, mach * np.sqrt(gamma * T1), 0.0, 0.0, T1)

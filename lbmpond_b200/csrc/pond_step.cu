@@ -14,6 +14,7 @@
 #include "pond_step_d3q27.cuh"
 #include "pond_step_point.cuh"
 #include "pond_step_weno3d.cuh"
+#include "pond_step_d3q125_weno_tile.cuh"
 
 namespace pond {
 
@@ -270,6 +271,16 @@ template <typename R> static int launch_typed(pond_ctx* c, const void* const* in
       const unsigned grd = (unsigned)((a.N + per - 1) / per);
       if (fix) w3d::pull_weno3d_kernel<POND_D3Q27, R, true><<<grd, w3d::THREADS, 0, s>>>(a);
       else w3d::pull_weno3d_kernel<POND_D3Q27, R, false><<<grd, w3d::THREADS, 0, s>>>(a);
+    } else if (std::is_same<R, float>::value && fix) {  // staged tile (float32, row through the departure point)
+      if constexpr (std::is_same<R, float>::value) {
+        const size_t smem = sizeof(d125w::Smem);
+        e = cudaFuncSetAttribute(d125w::pull_d3q125_weno_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+        const dim3 grd((a.nx + d125w::TX - 1) / d125w::TX, (a.ny + d125w::TY - 1) / d125w::TY,
+                       (a.nz + d125w::TZ - 1) / d125w::TZ);
+        d125w::pull_d3q125_weno_tile_kernel<<<grd, d125w::THREADS, smem, s>>>(a);
+      }
     } else {
       const long long per = (long long)w3d::WARPS * w3d::Geo<POND_D3Q125>::NPW;
       const unsigned grd = (unsigned)((a.N + per - 1) / per);

@@ -170,6 +170,93 @@ __device__ __forceinline__ double weno5_blend(const double S[3], const double u[
 
 __device__ __forceinline__ int clamp_off(int o) { return o < -MAXOFF ? -MAXOFF : (o > MAXOFF ? MAXOFF : o); }
 
+// The three candidate sums S[s][i2] and the smoothness-row values U5[m][i2]
+// of this lane's populations (p, i2, k), every stencil site read from global
+// memory and transferred into the iterate's gauge (U, C) by the group.  All
+// 32 lanes call it together; `done` lanes contribute no window.  Windows
+// (relative offsets): x nodes bx .. bx+4 with candidate s on bx+s .. bx+s+2
+// (weights LX[s]), z nodes bz .. bz+2 (WZ), y nodes by[i2] .. by[i2]+2
+// (WY[i2]).  `work` counts the sites transferred (leader lane only).
+template <int LAT, typename R, bool kRowFix>
+__device__ __forceinline__ void accumulate_global(const StepArgs<R>& a, int x, int y, int z, bool done, int base,
+                                                  int p, int k, const R Uc[3], R invC, int bx, const R LX[3][3],
+                                                  int bz, const R WZ[3], const int by[Lattice<LAT>::Q1],
+                                                  const R WY[Lattice<LAT>::Q1][3], R S[3][Lattice<LAT>::Q1],
+                                                  R U5[5][Lattice<LAT>::Q1], unsigned long long& work, bool leader) {
+  constexpr int Q1 = Lattice<LAT>::Q1;
+  // the warp's union of windows (relative offsets)
+  int ylo = by[0], yhi = by[0];
+#pragma unroll
+  for (int i2 = 1; i2 < Q1; i2++) { ylo = min(ylo, by[i2]); yhi = max(yhi, by[i2]); }
+  const int wxl = __reduce_min_sync(0xffffffffu, done ? MAXOFF : bx);
+  const int wxh = __reduce_max_sync(0xffffffffu, done ? -MAXOFF : bx + 4);
+  const int wyl = __reduce_min_sync(0xffffffffu, done ? MAXOFF : ylo);
+  const int wyh = __reduce_max_sync(0xffffffffu, done ? -MAXOFF : yhi + 2);
+  const int wzl = __reduce_min_sync(0xffffffffu, done ? MAXOFF : bz);
+  const int wzh = __reduce_max_sync(0xffffffffu, done ? -MAXOFF : bz + 2);
+#pragma unroll
+  for (int s = 0; s < 3; s++)
+#pragma unroll
+    for (int i2 = 0; i2 < Q1; i2++) S[s][i2] = R(0);
+#pragma unroll
+  for (int m = 0; m < 5; m++)
+#pragma unroll
+    for (int i2 = 0; i2 < Q1; i2++) U5[m][i2] = R(0);
+  if (!done && leader) work += (unsigned long long)(wxh - wxl + 1) * (wyh - wyl + 1) * (wzh - wzl + 1);
+  for (int oz = wzl; oz <= wzh; oz++) {
+    const int jz = oz - bz;
+    const R wz = jz == 0 ? WZ[0] : jz == 1 ? WZ[1] : jz == 2 ? WZ[2] : R(0);
+    for (int oy = wyl; oy <= wyh; oy++) {
+      for (int ox = wxl; ox <= wxh; ox++) {
+        const Site st = resolve_site(x + ox, y + oy, z + oz, a.nx, a.ny, a.nz, a.bc);
+        R fT[Q1];
+        site_transfer<LAT, R>(a, st, base, p, k, Uc, invC, fT);
+        const int jx = ox - bx;
+        R lxs[3];
+#pragma unroll
+        for (int s = 0; s < 3; s++) {
+          const int j = jx - s;
+          lxs[s] = j == 0 ? LX[s][0] : j == 1 ? LX[s][1] : j == 2 ? LX[s][2] : R(0);
+        }
+#pragma unroll
+        for (int i2 = 0; i2 < Q1; i2++) {
+          const int jy = oy - by[i2];
+          const R wy = jy == 0 ? WY[i2][0] : jy == 1 ? WY[i2][1] : jy == 2 ? WY[i2][2] : R(0);
+          const R v = wy * wz * fT[i2];
+#pragma unroll
+          for (int s = 0; s < 3; s++) S[s][i2] = fma(lxs[s], v, S[s][i2]);
+          if (kRowFix && jy == 0 && jz == 0) {
+#pragma unroll
+            for (int m = 0; m < 5; m++) U5[m][i2] = (jx == m) ? fT[i2] : U5[m][i2];
+          }
+        }
+      }
+    }
+  }
+  if (!kRowFix) {
+    // the reference's smoothness row (:783): nodes fx-2 .. fx+2 at y = z = fx
+    // (absolute coordinates; fx = x + bx + 2 for this lane's x-class)
+    const int fl = __reduce_min_sync(0xffffffffu, done ? MAXOFF : bx + 2);
+    const int fh = __reduce_max_sync(0xffffffffu, done ? -MAXOFF : bx + 2);
+    if (!done && leader) work += 5ull * (fh - fl + 1);
+    for (int df = fl; df <= fh; df++) {
+      const int F = x + df;
+#pragma unroll 1
+      for (int m = 0; m < 5; m++) {
+        const Site st = resolve_site(F - 2 + m, F, F, a.nx, a.ny, a.nz, a.bc);
+        R fT[Q1];
+        site_transfer<LAT, R>(a, st, base, p, k, Uc, invC, fT);
+        if (df == bx + 2) {
+#pragma unroll
+          for (int i2 = 0; i2 < Q1; i2++)
+#pragma unroll
+            for (int mm = 0; mm < 5; mm++) U5[mm][i2] = (mm == m) ? fT[i2] : U5[mm][i2];
+        }
+      }
+    }
+  }
+}
+
 // The WENO5 step.  kRowFix: smoothness row through the departure point.
 template <int LAT, typename R, bool kRowFix>
 __global__ void __launch_bounds__(THREADS) pull_weno3d_kernel(StepArgs<R> a) {
@@ -237,78 +324,9 @@ __global__ void __launch_bounds__(THREADS) pull_weno3d_kernel(StepArgs<R> a) {
       by[i2] = clamp_off((int)fyd - y);
       lagr_weights<3, R>(crdy - fyd, WY[i2]);
     }
-    // the warp's union of windows (relative offsets)
-    int ylo = by[0], yhi = by[0];
-#pragma unroll
-    for (int i2 = 1; i2 < Q1; i2++) { ylo = min(ylo, by[i2]); yhi = max(yhi, by[i2]); }
-    const int wxl = __reduce_min_sync(0xffffffffu, done ? MAXOFF : bx);
-    const int wxh = __reduce_max_sync(0xffffffffu, done ? -MAXOFF : bx + 4);
-    const int wyl = __reduce_min_sync(0xffffffffu, done ? MAXOFF : ylo);
-    const int wyh = __reduce_max_sync(0xffffffffu, done ? -MAXOFF : yhi + 2);
-    const int wzl = __reduce_min_sync(0xffffffffu, done ? MAXOFF : bz);
-    const int wzh = __reduce_max_sync(0xffffffffu, done ? -MAXOFF : bz + 2);
     R S[3][Q1], U5[5][Q1];
-#pragma unroll
-    for (int s = 0; s < 3; s++)
-#pragma unroll
-      for (int i2 = 0; i2 < Q1; i2++) S[s][i2] = R(0);
-#pragma unroll
-    for (int m = 0; m < 5; m++)
-#pragma unroll
-      for (int i2 = 0; i2 < Q1; i2++) U5[m][i2] = R(0);
-    if (!done && lane == base) work += (unsigned long long)(wxh - wxl + 1) * (wyh - wyl + 1) * (wzh - wzl + 1);
-    for (int oz = wzl; oz <= wzh; oz++) {
-      const int jz = oz - bz;
-      const R wz = jz == 0 ? WZ[0] : jz == 1 ? WZ[1] : jz == 2 ? WZ[2] : R(0);
-      for (int oy = wyl; oy <= wyh; oy++) {
-        for (int ox = wxl; ox <= wxh; ox++) {
-          const Site st = resolve_site(x + ox, y + oy, z + oz, a.nx, a.ny, a.nz, a.bc);
-          R fT[Q1];
-          site_transfer<LAT, R>(a, st, base, p, k, Uc, invC, fT);
-          const int jx = ox - bx;
-          R lxs[3];
-#pragma unroll
-          for (int s = 0; s < 3; s++) {
-            const int j = jx - s;
-            lxs[s] = j == 0 ? LX[s][0] : j == 1 ? LX[s][1] : j == 2 ? LX[s][2] : R(0);
-          }
-#pragma unroll
-          for (int i2 = 0; i2 < Q1; i2++) {
-            const int jy = oy - by[i2];
-            const R wy = jy == 0 ? WY[i2][0] : jy == 1 ? WY[i2][1] : jy == 2 ? WY[i2][2] : R(0);
-            const R v = wy * wz * fT[i2];
-#pragma unroll
-            for (int s = 0; s < 3; s++) S[s][i2] = fma(lxs[s], v, S[s][i2]);
-            if (kRowFix && jy == 0 && jz == 0) {
-#pragma unroll
-              for (int m = 0; m < 5; m++) U5[m][i2] = (jx == m) ? fT[i2] : U5[m][i2];
-            }
-          }
-        }
-      }
-    }
-    if (!kRowFix) {
-      // the reference's smoothness row (:783): nodes fx-2 .. fx+2 at y = z = fx
-      // (absolute coordinates; fx = x + bx + 2 for this lane's x-class)
-      const int fl = __reduce_min_sync(0xffffffffu, done ? MAXOFF : bx + 2);
-      const int fh = __reduce_max_sync(0xffffffffu, done ? -MAXOFF : bx + 2);
-      if (!done && lane == base) work += 5ull * (fh - fl + 1);
-      for (int df = fl; df <= fh; df++) {
-        const int F = x + df;
-#pragma unroll 1
-        for (int m = 0; m < 5; m++) {
-          const Site st = resolve_site(F - 2 + m, F, F, a.nx, a.ny, a.nz, a.bc);
-          R fT[Q1];
-          site_transfer<LAT, R>(a, st, base, p, k, Uc, invC, fT);
-          if (df == bx + 2) {
-#pragma unroll
-            for (int i2 = 0; i2 < Q1; i2++)
-#pragma unroll
-              for (int mm = 0; mm < 5; mm++) U5[mm][i2] = (mm == m) ? fT[i2] : U5[mm][i2];
-          }
-        }
-      }
-    }
+    accumulate_global<LAT, R, kRowFix>(a, x, y, z, done, base, p, k, Uc, invC, bx, LX, bz, WZ, by, WY, S, U5, work,
+                                       lane == base);
     // blend, calcMoments (structs.cuh:315-342) and isConv (steps.cu:58-75) in float64
     R acc[Q1];
     double mv[5] = {0, 0, 0, 0, 0};

@@ -18,13 +18,15 @@ pytestmark = pytest.mark.gpu
 WENO5, WENO5_ROW, FIXED3 = 8, 11, 6
 
 
-def _pair(orc, pond, lat, shape, interp, precision, tau=0.8, nsteps=2, seed=4, du=0.01, bc=(0, 0, 0), inflow=None):
+def _pair(orc, pond, lat, shape, interp, precision, tau=0.8, nsteps=2, seed=4, du=0.01, bc=(0, 0, 0), inflow=None,
+          ux_shift=0.0):
     # D3Q27 (TLat = 1/3) at T = 0.2: at lower temperatures some float64 nodes of
     # the oracle cycle at the iteration cap on these random non-equilibrium states
     T0 = 0.2 if lat == 1 else 0.1
     rho, g = smooth_state(shape, 3, seed=seed, modes=1, du=du, T0=T0)
     if inflow is not None:  # a flow along x into the box
         g[0] += inflow[1]
+    g[0] += ux_shift
     st = orc.State(perturbed_populations(orc, lat, rho, g, seed=seed, eps=0.01), rho, g)
     names = {0: "periodic", 1: "clamp", 2: "mirror", 3: "inflow"}
     with pond.Solver(lattice=lat, shape=shape, interp=interp, precision=precision, tau=tau,
@@ -52,6 +54,15 @@ def test_weno3d_matches_oracle(orc, pond, lat, shape, interp, seed, precision):
     _compare(out, ref, TOL[precision], f"lat {lat} {shape} interp {interp} {precision}")
     if precision == "fp64":
         assert d["niter_max"] == int(niter.max()) and d["nonconverged"] == 0
+
+
+@pytest.mark.parametrize("shift", [0.7, -0.75])
+def test_weno_tile_fast_flow_matches_oracle(orc, pond, shift):
+    """D3Q125 WENO5 (row through the departure point) in float32 runs the
+    staged tile; with |u_x| + 2.86 sqrt(T) > 1.5 some x windows leave the
+    tile's halo and those iterations read global memory instead."""
+    out, ref, niter, d = _pair(orc, pond, 2, (9, 5, 4), WENO5_ROW, "fp32", seed=5, ux_shift=shift)
+    _compare(out, ref, TOL["fp32"], f"fast flow {shift}")
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
