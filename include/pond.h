@@ -160,6 +160,14 @@ int pond_get_fields(pond_ctx* ctx, double* rho, double* ux, double* uy, double* 
    are f_i = rho w_i in the gauge (u, T) (set_base, lbpack.cu:15-21), with
    energy populations at their equilibrium when the context carries them. */
 int pond_set_inflow(pond_ctx* ctx, double rho, double ux, double uy, double uz, double T);
+/* Convergence tolerance of the gauge alone: the iteration's test on u and T
+   uses |new-old| < tol_abs + tol_rel*|new| with these values, the test on
+   every population keeps params.tol_abs / tol_rel.  The reference uses one
+   pair for both (isConv, steps.cu:58-75); a float32 context can so test the
+   float64 gauge residual below the float32 rounding floor of the
+   populations.  A negative value restores the params' pair.  Not used by the
+   batched 1D mode. */
+int pond_set_gauge_tolerance(pond_ctx* ctx, double tol_abs, double tol_rel);
 /* advance nsteps steps (calcStep without drop/diagnostics printing) */
 int pond_step(pond_ctx* ctx, int nsteps);
 int pond_diagnostics(pond_ctx* ctx, pond_diag* out);

@@ -159,6 +159,11 @@ class Solver:
         """State of the ghost node of ``"inflow"`` axes (equilibrium populations)."""
         _lib.check(self._L.pond_set_inflow(self._ctx, float(rho), float(ux), float(uy), float(uz), float(T)))
 
+    def set_gauge_tolerance(self, tol_abs, tol_rel=0.0):
+        """A separate convergence tolerance on u and T (the populations keep
+        the Solver's); negative values restore the Solver's pair."""
+        _lib.check(self._L.pond_set_gauge_tolerance(self._ctx, float(tol_abs), float(tol_rel)))
+
     def step(self, n=1):
         _lib.check(self._L.pond_step(self._ctx, int(n)))
 

@@ -66,6 +66,7 @@ SIGNATURES = {
     "pond_get_fields": (ctypes.c_int, [_vp, _dp, _dp, _dp, _dp, _dp]),
     "pond_step": (ctypes.c_int, [_vp, ctypes.c_int]),
     "pond_set_inflow": (ctypes.c_int, [_vp] + [ctypes.c_double] * 5),
+    "pond_set_gauge_tolerance": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double]),
     "pond_diagnostics": (ctypes.c_int, [_vp, ctypes.POINTER(PondDiag)]),
     "pond_set_clock": (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.c_double, ctypes.c_double]),
     "pond_set_strict": (ctypes.c_int, [_vp, ctypes.c_int]),

@@ -536,6 +536,16 @@ int pond_set_inflow(pond_ctx* c, double rho, double ux, double uy, double uz, do
   return POND_OK;
 }
 
+int pond_set_gauge_tolerance(pond_ctx* c, double tol_abs, double tol_rel) {
+  if (!c) return set_error(POND_ERR_ARG, "null argument");
+  if (std::isnan(tol_abs) || std::isnan(tol_rel) || std::isinf(tol_abs) || std::isinf(tol_rel))
+    return set_error(POND_ERR_ARG, "gauge tolerances must be finite");
+  const bool off = tol_abs < 0 || tol_rel < 0;
+  c->tolg_abs = off ? -1 : tol_abs;
+  c->tolg_rel = off ? -1 : tol_rel;
+  return POND_OK;
+}
+
 int pond_step(pond_ctx* c, int nsteps) {
   if (!c) return set_error(POND_ERR_ARG, "null context");
   { const int ps = pipe_drain(c); if (ps != POND_OK) return ps; }

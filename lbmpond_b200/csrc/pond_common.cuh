@@ -173,7 +173,8 @@ template <typename R> struct StepArgs {
   long long N;
   int bc[3];
   double dtau;
-  double tol_abs, tol_rel;
+  double tol_abs, tol_rel;    // isConv on every population
+  double tolg_abs, tolg_rel;  // isConv on the gauge u, T (the reference uses tol_abs, tol_rel for both)
   int max_iter;
   double kdx;  // 0.5 * dx*dy*dz / (8 pi^3) with dx = 2 pi / Nx (diagn.cu:14-18)
   // energy populations of the double-distribution extension (D1Q5), or null

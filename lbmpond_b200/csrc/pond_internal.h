@@ -61,6 +61,8 @@ struct pond_ctx {
   // ghost state of POND_BC_INFLOW axes (pond_set_inflow): rho, u_x, u_y, u_z, T
   double inflow[5] = {1, 0, 0, 0, 1};
   bool have_inflow = false;
+  // separate convergence tolerance on the gauge u, T (pond_set_gauge_tolerance); < 0: params' tol_abs / tol_rel
+  double tolg_abs = -1, tolg_rel = -1;
   // time-step adaptation after every step (update.cu:121-123)
   bool dt_adapt = false;
   int adapt_hi = 1000, adapt_lo = 4;

@@ -171,6 +171,7 @@ extern "C" int pond_step_noalloc(const pond_params* p, const float* f_in, const 
   for (int k = 0; k < 3; k++) a.bc[k] = p->bc[k];
   a.dtau = 1.0 / p->tau;
   a.tol_abs = p->tol_abs; a.tol_rel = p->tol_rel;
+  a.tolg_abs = p->tol_abs; a.tolg_rel = p->tol_rel;
   a.max_iter = p->max_iter;
   const double PI = 3.14159265358979323846;
   a.kdx = 0.5 / (8 * PI * PI * PI) * (2 * PI / p->Nx) * (2 * PI / p->Ny) * (2 * PI / p->Nz);

@@ -202,6 +202,8 @@ template <typename R> static int launch_typed(pond_ctx* c, const void* const* in
   for (int k = 0; k < 3; k++) a.bc[k] = c->p.bc[k];
   a.dtau = 1.0 / c->p.tau;
   a.tol_abs = c->p.tol_abs; a.tol_rel = c->p.tol_rel;
+  a.tolg_abs = c->tolg_abs >= 0 ? c->tolg_abs : c->p.tol_abs;
+  a.tolg_rel = c->tolg_rel >= 0 ? c->tolg_rel : c->p.tol_rel;
   a.max_iter = c->p.max_iter;
   a.kdx = kdx_of(c);
   a.mask = c->mask[0] ? c->mask[c->mask_cur] : nullptr;

@@ -167,10 +167,10 @@ __global__ void __launch_bounds__(128) pull_1d_energy_kernel(StepArgs<R> a) {
       }
       double Tn = (esum - m0 * m0 - m1 * m1 - m2 * m2) / (L::Dim + a.dof);
       if (Tn < 0) Tn = T;  // steps.cu:475
-      bool ok = !(fabs(m0 - U[0]) >= a.tol_abs + a.tol_rel * fabs(m0)) &&
-                !(fabs(m1 - U[1]) >= a.tol_abs + a.tol_rel * fabs(m1)) &&
-                !(fabs(m2 - U[2]) >= a.tol_abs + a.tol_rel * fabs(m2)) &&
-                !(fabs(Tn - T) >= a.tol_abs + a.tol_rel * fabs(Tn));
+      bool ok = !(fabs(m0 - U[0]) >= a.tolg_abs + a.tolg_rel * fabs(m0)) &&
+                !(fabs(m1 - U[1]) >= a.tolg_abs + a.tolg_rel * fabs(m1)) &&
+                !(fabs(m2 - U[2]) >= a.tolg_abs + a.tolg_rel * fabs(m2)) &&
+                !(fabs(Tn - T) >= a.tolg_abs + a.tolg_rel * fabs(Tn));
 #pragma unroll
       for (int k = 0; k < Q; k++) {
         const double nf = fnew[k], of = f0[k], nh = hnew[k], oh = h0[k];

@@ -372,8 +372,8 @@ __global__ void __launch_bounds__(THREADS, 1) pull_d3q125_weno_tile_kernel(StepA
         if (Tn < 0) Tn = Tc;  // steps.cu:475
         bool ok = true;
 #pragma unroll
-        for (int q = 0; q < 3; q++) ok = ok && !(fabs(m[q] - U[q]) >= a.tol_abs + a.tol_rel * fabs(m[q]));
-        ok = ok && !(fabs(Tn - Tc) >= a.tol_abs + a.tol_rel * fabs(Tn));
+        for (int q = 0; q < 3; q++) ok = ok && !(fabs(m[q] - U[q]) >= a.tolg_abs + a.tolg_rel * fabs(m[q]));
+        ok = ok && !(fabs(Tn - Tc) >= a.tolg_abs + a.tolg_rel * fabs(Tn));
         if (worker)
 #pragma unroll
           for (int iy = 0; iy < 5; iy++) {

@@ -172,9 +172,9 @@ __global__ void __launch_bounds__(128) pull_d3q27_energy_kernel(StepArgs<R> a) {
       }
       double Tn = (esum - m[0] * m[0] - m[1] * m[1] - m[2] * m[2]) / (L::Dim + a.dof);
       if (Tn < 0) Tn = T;  // steps.cu:475
-      bool ok = !(fabs(Tn - T) >= a.tol_abs + a.tol_rel * fabs(Tn));
+      bool ok = !(fabs(Tn - T) >= a.tolg_abs + a.tolg_rel * fabs(Tn));
 #pragma unroll
-      for (int k = 0; k < 3; k++) ok = ok && !(fabs(m[k] - U[k]) >= a.tol_abs + a.tol_rel * fabs(m[k]));
+      for (int k = 0; k < 3; k++) ok = ok && !(fabs(m[k] - U[k]) >= a.tolg_abs + a.tolg_rel * fabs(m[k]));
 #pragma unroll
       for (int t = 0; t < Q; t++) {
         const double nf = acc[t], of = f0[t], nh = acch[t], oh = h0[t];

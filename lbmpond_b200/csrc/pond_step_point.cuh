@@ -218,8 +218,8 @@ __device__ __forceinline__ bool moments_and_test(const StepArgs<R>& a, const R a
   if (Tn < 0) Tn = T;
   bool ok = true;
 #pragma unroll
-  for (int k = 0; k < 3; k++) ok = ok && !(fabs(m[k] - U[k]) >= a.tol_abs + a.tol_rel * fabs(m[k]));
-  ok = ok && !(fabs(Tn - T) >= a.tol_abs + a.tol_rel * fabs(Tn));
+  for (int k = 0; k < 3; k++) ok = ok && !(fabs(m[k] - U[k]) >= a.tolg_abs + a.tolg_rel * fabs(m[k]));
+  ok = ok && !(fabs(Tn - T) >= a.tolg_abs + a.tolg_rel * fabs(Tn));
 #pragma unroll
   for (int t = 0; t < Q; t++) {
     const double nv = acc[t], ov = f0[t];

@@ -362,8 +362,8 @@ __global__ void __launch_bounds__(THREADS) pull_weno3d_kernel(StepArgs<R> a) {
     if (Tn < 0) Tn = T;  // steps.cu:475
     bool ok = true;
 #pragma unroll
-    for (int q = 0; q < 3; q++) ok = ok && !(fabs(m[q] - U[q]) >= a.tol_abs + a.tol_rel * fabs(m[q]));
-    ok = ok && !(fabs(Tn - T) >= a.tol_abs + a.tol_rel * fabs(Tn));
+    for (int q = 0; q < 3; q++) ok = ok && !(fabs(m[q] - U[q]) >= a.tolg_abs + a.tolg_rel * fabs(m[q]));
+    ok = ok && !(fabs(Tn - T) >= a.tolg_abs + a.tolg_rel * fabs(Tn));
 #pragma unroll
     for (int i2 = 0; i2 < Q1; i2++) {
       const double nv = acc[i2], ov = f0[i2];

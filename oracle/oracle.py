@@ -45,6 +45,7 @@ class _Params(ctypes.Structure):
         ("nthreads", ctypes.c_int),
         ("dof", ctypes.c_double),
         ("inflow", ctypes.c_double * 5),
+        ("tolg", ctypes.c_double * 2),
     ]
 
 
@@ -199,11 +200,12 @@ def base_state(lattice: int, rho, ux, uy, uz, T) -> State:
 
 
 def step(state: State, lattice: int, shape, interp=None, tau=0.9, tol_abs=1e-12, tol_rel=1e-10,
-         max_iter=100, bc=(BC_PERIODIC,) * 3, guess=None, nthreads=0, dof=None, inflow=None):
+         max_iter=100, bc=(BC_PERIODIC,) * 3, guess=None, nthreads=0, dof=None, inflow=None, tolg=None):
     """One pull step; returns (new_state, niter[N], nonconverged_count).  A
     state with energy populations (``state.h``) steps with the
     double-distribution extension and needs ``dof``.  ``inflow`` = (rho,
-    u_x, u_y, u_z, T) of the ghost node of BC_INFLOW axes."""
+    u_x, u_y, u_z, T) of the ghost node of BC_INFLOW axes; ``tolg`` = (abs,
+    rel) tolerance of the gauge's convergence test (default: tol_abs, tol_rel)."""
     L = lib()
     nx, ny, nz = shape
     N = nx * ny * nz
@@ -215,7 +217,8 @@ def step(state: State, lattice: int, shape, interp=None, tau=0.9, tol_abs=1e-12,
         raise ValueError("a state with energy populations needs dof")
     p = _Params(lattice, interp, nx, ny, nz, (ctypes.c_int * 3)(*bc), tau, tol_abs, tol_rel,
                 max_iter, nthreads, float(dof) if ddf else 0.0,
-                (ctypes.c_double * 5)(*(inflow if inflow is not None else (1.0, 0.0, 0.0, 0.0, 1.0))))
+                (ctypes.c_double * 5)(*(inflow if inflow is not None else (1.0, 0.0, 0.0, 0.0, 1.0))),
+                (ctypes.c_double * 2)(*(tolg if tolg is not None else (-1.0, -1.0))))
     f_in = np.ascontiguousarray(state.f, dtype=np.float64)
     r_in = np.ascontiguousarray(state.rho, dtype=np.float64)
     g_in = np.ascontiguousarray(state.g, dtype=np.float64)
@@ -247,7 +250,8 @@ def _u8p(a):
 
 def _mesh_params(nx, interp=LAGR2, tau=0.9, tol_abs=1e-12, tol_rel=1e-10, max_iter=100, nthreads=0):
     return _Params(D1Q5, interp, nx, 1, 1, (ctypes.c_int * 3)(BC_PERIODIC, BC_PERIODIC, BC_PERIODIC), tau,
-                   tol_abs, tol_rel, max_iter, nthreads, 0.0)
+                   tol_abs, tol_rel, max_iter, nthreads, 0.0, (ctypes.c_double * 5)(1.0, 0.0, 0.0, 0.0, 1.0),
+                   (ctypes.c_double * 2)(-1.0, -1.0))
 
 
 def step_mesh(state: State, nx: int, interp=GAP2, mask=None, pos=None, tau=0.9, tol_abs=1e-12, tol_rel=1e-10,

@@ -290,9 +290,12 @@ void calc_moments(const Lattice& L, Cell& c, const double (*vi)[3]) {
 }
 
 // steps.cu:58-75 isConv
-bool is_conv(const Lattice& L, const Cell& cnew, const Cell& cold, double ea, double er, bool ddf = false) {
+// (ga, gr: the gauge's own tolerance, an extension; the reference tests u, T
+// with ea, er like the populations)
+bool is_conv(const Lattice& L, const Cell& cnew, const Cell& cold, double ea, double er, bool ddf, double ga,
+             double gr) {
   for (int k = 0; k < 4; k++)
-    if (std::fabs(cnew.uT[k] - cold.uT[k]) >= ea + er * std::fabs(cnew.uT[k])) return false;
+    if (std::fabs(cnew.uT[k] - cold.uT[k]) >= ga + gr * std::fabs(cnew.uT[k])) return false;
   for (int i = 0; i < L.Q; i++)
     if (std::fabs(cnew.f[i] - cold.f[i]) >= ea + er * std::fabs(cnew.f[i])) return false;
   if (ddf)  // the energy populations converge like the others
@@ -644,7 +647,12 @@ int pull_node(const Domain& D, const orc_params& P, int64_t x, int64_t y, int64_
       cnew.uT[3] = (e - cnew.uT[0] * cnew.uT[0] - cnew.uT[1] * cnew.uT[1] - cnew.uT[2] * cnew.uT[2]) / (L.Dim + dof);
     }
     if (cnew.uT[3] < 0) cnew.uT[3] = c0.uT[3];  // steps.cu:475-478
-    if (is_conv(L, cnew, c0, P.tol_abs, P.tol_rel, ddf)) { c0 = cnew; conv = true; break; }
+    const bool gsep = P.tolg[0] >= 0 && P.tolg[1] >= 0;
+    if (is_conv(L, cnew, c0, P.tol_abs, P.tol_rel, ddf, gsep ? P.tolg[0] : P.tol_abs, gsep ? P.tolg[1] : P.tol_rel)) {
+      c0 = cnew;
+      conv = true;
+      break;
+    }
     c0 = cnew;
   }
   const double dtau = 1.0 / P.tau;

@@ -46,6 +46,7 @@ typedef struct {
   int nthreads;       /* 0 = OpenMP default */
   double dof;         /* double-distribution extension: extra degrees of freedom (orc_step_ddf) */
   double inflow[5];   /* state of the ORC_BC_INFLOW ghost node: rho, u_x, u_y, u_z, T */
+  double tolg[2];     /* abs, rel tolerance of the test on u, T; negative: tol_abs, tol_rel */
 } orc_params;
 
 int    orc_q(int lattice);

@@ -304,3 +304,28 @@ def test_twenty_steps_l1_and_drift(orc, pond, precision, l1_tol):
     de_gpu = (d1["enrg"] - d0["enrg"]) / d0["enrg"]
     de_ref = (e1["enrg"] - e0["enrg"]) / e0["enrg"]
     assert abs(dm_gpu - dm_ref) <= 50 * l1_tol and abs(de_gpu - de_ref) <= 50 * l1_tol
+
+
+@pytest.mark.parametrize("lat,shape,interp", [(1, (9, 7, 5), 4), (0, (97, 1, 1), 8), (2, (9, 6, 5), 6)])
+def test_gauge_tolerance_matches_oracle(orc, pond, lat, shape, interp):
+    """pond_set_gauge_tolerance: the test on u, T uses its own pair (here
+    1e-13 + 1e-12|v|) while every population keeps the context's (1e-9 +
+    1e-8|f|); float64 against the oracle with the same split."""
+    st = _state(orc, lat, shape, "smooth", 7)
+    with pond.Solver(lattice=lat, shape=shape, interp=interp, precision="fp64", tau=0.8, tol_abs=1e-9,
+                     tol_rel=1e-8) as s:
+        s.set_state(st.rho, st.g, f=st.f)
+        s.set_gauge_tolerance(1e-13, 1e-12)
+        s.keep_niter(True)
+        s.step(1)
+        out = s.get_state()
+        ni = s.niter()
+    ref, niter, nc = orc.step(st, lat, shape, interp=interp, tau=0.8, tol_abs=1e-9, tol_rel=1e-8,
+                              tolg=(1e-13, 1e-12))
+    assert nc == 0
+    _compare(out, ref, TOL["fp64"], "gauge tolerance")
+    assert np.array_equal(ni, niter)
+    loose, niter_loose, _ = orc.step(st, lat, shape, interp=interp, tau=0.8, tol_abs=1e-9, tol_rel=1e-8)
+    assert niter.sum() >= niter_loose.sum()  # the tighter gauge test iterates more (D3Q125 here: as much)
+    if lat != 2:
+        assert niter.sum() > niter_loose.sum()
