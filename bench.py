@@ -142,9 +142,54 @@ def _oracle_sample(m, spin, warmup, steps):
     return m ** 3 / dt / 1e6, dt, float(np.mean(it)), O.max_threads()
 
 
+SAMPLE = os.path.join(ROOT, "tests", "golden", "bench", "sphere256_blocks.npz")
+
+
+def _oracle_blocks(warmup, steps):
+    """The FP64 oracle (restated reference step, all host threads) on blocks
+    cut out of the benchmark's own spun-up 256^3 state (tests/golden/bench,
+    made by tests/golden/make_cpu_sample.py): every pass steps each block
+    once from the stored state (zero-gradient block faces, the benchmark's
+    tau and tolerance), so each timed pass does the per-node work of the
+    timed GPU steps.  Returns (MLUPS, s per pass, iterations per node, the
+    GPU's iterations on the same nodes, threads, description)."""
+    from oracle import oracle as O
+    O.build()
+    z = np.load(SAMPLE)
+    e = int(z["edge"])
+    blocks = [O.State(z["f"][:, b].astype(np.float64), z["rho"][b].astype(np.float64),
+                      z["g"][:, b].astype(np.float64)) for b in range(z["rho"].shape[0])]
+    nodes = len(blocks) * e ** 3
+
+    def one_pass():
+        it = 0
+        for st in blocks:
+            _, niter, _ = O.step(st, 1, (e, e, e), tau=TAU, tol_abs=TOL_ABS, tol_rel=TOL_REL,
+                                 bc=(O.BC_CLAMP,) * 3)
+            it += int(niter.sum())
+        return it / nodes
+
+    for _ in range(warmup):
+        one_pass()
+    t0 = time.perf_counter()
+    its = [one_pass() for _ in range(steps)]
+    dt = (time.perf_counter() - t0) / max(steps, 1)
+    desc = (f"{len(blocks)} blocks of {e}^3 nodes cut from the 256^3 state after {int(z['spinup'])} spin-up "
+            f"steps (seeded positions; the GPU iterates {float(z['niter_gpu'].mean()):.2f} times per node on them, "
+            f"{float(z['niter_mean_domain']):.2f} over the whole box), each block stepped once per pass with "
+            f"zero-gradient faces")
+    return nodes / dt / 1e6, dt, float(np.mean(its)), float(z["niter_gpu"].mean()), O.max_threads(), desc
+
+
 def cpu_baseline(spinup=150, m=24):
-    """FP64 oracle on a bounded sample of the same problem at the same stage
-    of the blast (about 10-30 s of host time)."""
+    """FP64 oracle on a bounded sample of the same workload at the same stage
+    of the run (about 10-30 s of host time): the blocks of the spun-up state
+    when their file is present, else a coarse re-simulation."""
+    if os.path.exists(SAMPLE):
+        v, dt, it, it_gpu, cores, desc = _oracle_blocks(1, 3)
+        return {"value": v, "unit": "MLUPS", "cores": cores, "kind": "port",
+                "sample": f"{desc}; 3 timed passes of {dt:.2f} s on the FP64 oracle, {it:.2f} iterations per node",
+                "niter_mean": it, "niter_mean_gpu_same_nodes": it_gpu}
     spin = round(spinup * m / 256)
     v, dt, it, cores = _oracle_sample(m, spin, 0, 2)
     return {"value": v, "unit": "MLUPS", "cores": cores, "kind": "port",
@@ -153,29 +198,74 @@ def cpu_baseline(spinup=150, m=24):
 
 
 # ------------------------------------------------------------------ reference kernels on the GPU
-def reference_cuda(n=64):
-    """The reference's own PonDstep (FP64 and FP32 builds), kernel time only."""
-    from tests.golden.make_golden import read_state, write_state
-    out = {}
-    rho, g = sphere_state(n)
+REF_TOL = (1e-12, 1e-10)  # isConv of the reference's build (steps.cu:62-63), both precisions
+# (precision, grid, steps, timed steps): the reference's USE_DOUBLE build on the sphere
+# problem at 64^3 from the initial condition through the benchmark's spin-up scaled to
+# the grid (round(150 * 64 / 256) = 38 steps), timing the last two; its USE_FLOAT
+# build at 32^3, one step from the initial condition (it never meets its tolerance in
+# float32, so every node runs the 100-iteration cap whatever the state)
+SAME_STATE = (("double", 64, 40, 2), ("float", 32, 1, 1))
+
+
+def reference_cuda():
+    """Reference arm: the reference's own PonDstep (built for sm_100a from its
+    sources by oracle/build_ref.sh), kernel time by CUDA events, on the
+    SAME_STATE runs; this library's arm times its kernels on the same runs."""
     from oracle import oracle as O
-    w = O.tables(1).w
-    f = w[:, None] * rho[None, :]
-    for prec in ("double", "float"):
+    from tests.golden.make_golden import read_niter_mean, read_state, write_state
+    out = {}
+    for prec, n, nsteps, timed in SAME_STATE:
         binary = os.path.join(ROOT, "oracle", "_ref", f"ref_pond_D3Q27_{prec}_{n}x{n}x{n}")
         if not os.path.exists(binary):
             out[prec] = None
             continue
+        rho, g = sphere_state(n)
+        f = O.tables(1).w[:, None] * rho[None, :]
         with tempfile.TemporaryDirectory() as td:
             fin, fout = os.path.join(td, "in"), os.path.join(td, "out")
             write_state(fin, f, rho, g, (n, n, n))
-            r = subprocess.run([binary, fin, fout, "2", repr(TAU)], capture_output=True, text=True, timeout=900)
+            r = subprocess.run([binary, fin, fout, str(nsteps), repr(TAU)], capture_output=True, text=True,
+                               timeout=900)
             if r.returncode != 0:
                 out[prec] = {"error": r.stderr[-300:]}
                 continue
             _, _, _, nmax, ms = read_state(fout, 27, (n, n, n))
-        out[prec] = {"ms_per_step": float(ms[-1]), "MLUPS": n ** 3 / (float(ms[-1]) / 1e3) / 1e6,
-                     "niter_max": nmax, "grid": f"{n}^3"}
+            im = read_niter_mean(fout, 27, (n, n, n))
+        t = float(np.mean(ms[-timed:]))
+        out[prec] = {"build": "USE_DOUBLE" if prec == "double" else "USE_FLOAT", "grid": f"{n}^3",
+                     "steps": nsteps, "timed_steps": timed, "tolerance": list(REF_TOL), "ms_per_step": t,
+                     "MLUPS": n ** 3 / t / 1e3, "niter_mean_last_step": im, "niter_max_last_step": nmax,
+                     "node_iterations_per_s": n ** 3 * im / (t / 1e3) if im else None}
+    return out
+
+
+def ours_same_state(local=0):
+    """This library's kernels on reference_cuda's runs: the same initial state
+    and step counts, float64 at the reference's tolerance, float32 at the
+    reference's tolerance and at the benchmark's."""
+    import lbmpond_b200 as pond
+    out = {}
+    for prec, n, nsteps, timed in SAME_STATE:
+        rho, g = sphere_state(n)
+        runs = [("fp64", REF_TOL)] if prec == "double" else [("fp32", REF_TOL)]
+        runs.append(("fp32", (TOL_ABS, TOL_REL)))
+        rec = {"grid": f"{n}^3", "steps": nsteps, "timed_steps": timed}
+        for p, tol in runs:
+            with pond.Solver(lattice="D3Q27", shape=(n, n, n), interp=pond.LAGR4, precision=p, tau=TAU,
+                             tol_abs=tol[0], tol_rel=tol[1], device=local) as s:
+                s.set_state(rho, g)
+                s.step(nsteps - timed)
+                ms = []
+                for _ in range(timed):
+                    s.step(1)
+                    ms.append(s.last_step_ms())
+                d = s.diagnostics()
+            t = float(np.mean(ms))
+            key = p + ("_reference_tolerance" if tol == REF_TOL else "_bench_tolerance")
+            rec[key] = {"tolerance": list(tol), "ms_per_step": t, "MLUPS": n ** 3 / t / 1e3,
+                        "niter_mean_last_step": d["niter_mean"], "niter_max_last_step": d["niter_max"],
+                        "node_iterations_per_s": n ** 3 * d["niter_mean"] / (t / 1e3)}
+        out[prec] = rec
     return out
 
 
@@ -240,6 +330,21 @@ def run_ours(args, rank, local, world, pg):
     plain = {"value": world * N / (ms_plain / 1e3) / 1e6, "ms_per_step": ms_plain,
              "iterations_mean": p1["niter_mean"], "iterations_max": p1["niter_max"],
              "nonconverged": p1["nonconverged"]}
+
+    # the same plain path with the convergence test of u and T at an absolute
+    # 1e-8 (float64 gauge residual), the populations' test at the float32 floor
+    gauge_tight = None
+    if args.gauge_tol > 0:
+        t = mk()
+        t.copy_state_from(snap)
+        t.set_gauge_tolerance(args.gauge_tol, 0.0)
+        ms_g, _, g1 = _timed_window(t, pg, args.steps, args.warmup)
+        ms_g = allmax(pg, ms_g)
+        t.close()
+        gauge_tight = {"value": world * N / (ms_g / 1e3) / 1e6, "ms_per_step": ms_g,
+                       "iterations_mean": g1["niter_mean"], "iterations_max": g1["niter_max"],
+                       "nonconverged": g1["nonconverged"],
+                       "tolerance": {"gauge": [args.gauge_tol, 0.0], "populations": [TOL_ABS, TOL_REL]}}
 
     # learned path from the same state
     learned = None
@@ -371,7 +476,7 @@ def run_ours(args, rank, local, world, pg):
                    "parallelism": "replicas" if world > 1 else "single",
                    "spinup_steps": args.spinup, "spinup_seconds": t_spin,
                    "timed_steps": f"{args.spinup + args.warmup + 1}..{args.spinup + args.warmup + args.steps}"},
-        "plain": plain, "learned": learned,
+        "plain": plain, "learned": learned, "plain_gauge_residual_1e8": gauge_tight,
         "speedup_learned_vs_plain": (learned["value"] / plain["value"]) if learned else None,
         "l1_vs_fp64": l1, "drift": drift,
         "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
@@ -388,52 +493,96 @@ def run_ours(args, rank, local, world, pg):
     return out
 
 
-def run_batch1d(steps=1000, nproblems=4096, pg=None, rank=0, world=1):
-    """The batched D1Q5 workload: `nproblems` seeded Riemann problems
-    (lengths uniform in [256, 4096], rho and p log-uniform in [0.1, 10], u
-    uniform in [-1, 1], jump at the midpoint), WENO5, tau 0.9, float32 with
-    float64 moments, `steps` steps in persistent graph-replayed launches of
-    50 steps after the autotuner picked the tile.  Problems whose state
-    became non-finite are counted (the float64 oracle diverges on the same
-    strong-jump problems).  Under several ranks the problems are split by
-    node count (strong scaling: the whole set is the job) and the time is the
-    slowest rank's."""
+def _batch_set(lengths, rho, u, T, steps, chunk, pg, world, label):
+    """Advance one problem set `steps` steps in graph-replayed launches of
+    `chunk` steps, after the autotuner picked the tile; after every launch the
+    state is read back (outside the timed launches) to record the step at
+    which each problem first holds a non-finite value.  Returns the rates over
+    all node updates and over the updates of problems still finite."""
     from lbmpond_b200 import replicas
-    from lbmpond_b200.batch import Batch, riemann_problems
-    import torch
-    lengths, rho, u, T = riemann_problems(nproblems, seed=0)
-    off = np.concatenate([[0], np.cumsum(lengths)])
-    mine = replicas.partition_problems(lengths, world)[rank]
-    sel = np.concatenate([np.arange(off[p], off[p + 1]) for p in mine])
-    lengths, rho, u, T = lengths[mine], rho[sel], u[sel], T[sel]
+    from lbmpond_b200.batch import Batch
     with Batch(lengths, interp=8, tau=0.9) as b:
         b.set_state(rho, u, T)
         tile, _ = b.autotune(probe_steps=5)
         b.set_state(rho, u, T)
         replicas.barrier(pg)
-        ms = replicas.max_over_ranks(pg, b.run(steps, steps_per_launch=50))
-        st = b.stats()
-        f, r, uu, tt = b.get_state()
-        fin = np.isfinite(f).all(0) & np.isfinite(r) & np.isfinite(uu) & np.isfinite(tt)
-        bad = int(sum(not fin[b.offsets[p]:b.offsets[p + 1]].all() for p in range(lengths.size)))
-        cap = 1 << 21
-        X = torch.empty((cap, 21), dtype=torch.float32, device="cuda")
-        Y = torch.empty((cap, 2), dtype=torch.float32, device="cuda")
-        b.set_state(rho, u, T)
-        b.set_pairs(X, Y, every=10, stride=16)
-        ms_pairs = replicas.max_over_ranks(pg, b.run(100, steps_per_launch=50))
-        pairs = b.pairs_written()
-        nodes = replicas.sum_over_ranks(pg, b.nodes)
-    niter = replicas.sum_over_ranks(pg, st["niter_sum"])
-    nonconv = replicas.sum_over_ranks(pg, st["nonconverged"])
-    return {"workload": f"{nproblems} D1Q5 Riemann problems, lengths U[256,4096] (seed 0), WENO5, {steps} steps",
-            "nodes": int(nodes), "MLUPS": nodes * steps / (ms / 1e3) / 1e6, "ms_per_step": ms / steps,
-            "n_gpus": world, "scaling": "strong (problems split across ranks)" if world > 1 else None,
-            "tile": {"threads": tile[0], "lane_cap": tile[1]}, "niter_mean": niter / (nodes * steps),
-            "nonconverged_frac": nonconv / (nodes * steps),
-            "nonfinite_problems": int(replicas.sum_over_ranks(pg, bad)),
-            "pairs": {"rows_per_100_steps": int(replicas.sum_over_ranks(pg, pairs)), "every": 10, "stride": 16,
-                      "ms_per_step_with_pairs": ms_pairs / 100}}
+        alive = np.full(lengths.size, steps, dtype=np.int64)  # steps each problem stayed finite
+        ms = 0.0
+        niter = nonconv = 0
+        for k0 in range(0, steps, chunk):
+            ms += b.run(min(chunk, steps - k0), steps_per_launch=chunk)
+            st = b.stats()
+            niter += st["niter_sum"]
+            nonconv += st["nonconverged"]
+            f, r, uu, tt = b.get_state()
+            fin = np.isfinite(f).all(0) & np.isfinite(r) & np.isfinite(uu) & np.isfinite(tt)
+            for p in np.nonzero(alive == steps)[0]:
+                if not fin[b.offsets[p]:b.offsets[p + 1]].all():
+                    alive[p] = k0  # diverged within this launch: count the launch as lost
+        nodes = b.nodes
+    ms = replicas.max_over_ranks(pg, ms)
+    upd = replicas.sum_over_ranks(pg, nodes * steps)
+    upd_fin = replicas.sum_over_ranks(pg, int((lengths.astype(np.int64) * alive).sum()))
+    dead = alive < steps
+    out = {"workload": label, "nodes": int(replicas.sum_over_ranks(pg, nodes)), "steps": steps,
+           "MLUPS": upd / (ms / 1e3) / 1e6, "MLUPS_finite_updates": upd_fin / (ms / 1e3) / 1e6,
+           "ms_per_step": ms / steps, "tile": {"threads": tile[0], "lane_cap": tile[1]},
+           "niter_mean": replicas.sum_over_ranks(pg, niter) / upd,
+           "nonconverged_frac": replicas.sum_over_ranks(pg, nonconv) / upd,
+           "nonfinite_problems": int(replicas.sum_over_ranks(pg, int(dead.sum()))),
+           "steps_to_divergence": {"resolution": chunk,
+                                   "quartiles": [float(q) for q in np.percentile(alive[dead], [25, 50, 75])]
+                                   if dead.any() else None}}
+    return out
+
+
+def run_batch1d(steps=1000, nproblems=4096, pg=None, rank=0, world=1):
+    """The batched D1Q5 workload: `nproblems` seeded Riemann problems
+    (lengths uniform in [256, 4096], rho and p log-uniform in [0.1, 10], u
+    uniform in [-1, 1], jump at the midpoint), WENO5, tau 0.9, float32 with
+    float64 moments, `steps` steps in persistent graph-replayed launches of
+    50 steps after the autotuner picked the tile.  The reference iteration
+    drives most of these problems non-finite (the float64 oracle diverges on
+    the same strong jumps), so the line also gives the rate over the node
+    updates of problems still finite and the steps to divergence, and the same
+    measurement on a well-posed companion set (density ratio <= 10,
+    temperature ratio <= 2, moderate velocities).  Under several ranks the
+    problems are split by node count (strong scaling: the whole set is the
+    job) and the time is the slowest rank's."""
+    from lbmpond_b200 import replicas
+    from lbmpond_b200.batch import Batch, riemann_problems, riemann_problems_moderate
+    import torch
+    out = None
+    for which in ("specified", "moderate"):
+        gen = riemann_problems if which == "specified" else riemann_problems_moderate
+        lengths, rho, u, T = gen(nproblems, seed=0)
+        off = np.concatenate([[0], np.cumsum(lengths)])
+        mine = replicas.partition_problems(lengths, world)[rank]
+        sel = np.concatenate([np.arange(off[p], off[p + 1]) for p in mine])
+        lengths, rho, u, T = lengths[mine], rho[sel], u[sel], T[sel]
+        label = (f"{nproblems} D1Q5 Riemann problems, lengths U[256,4096] (seed 0), WENO5, {steps} steps"
+                 if which == "specified" else
+                 f"{nproblems} moderate D1Q5 Riemann problems (density ratio <= 10, temperature ratio <= 2, "
+                 f"|u| <= 0.09, lattice T ~ 0.09), lengths U[256,4096] (seed 0), WENO5, {steps} steps")
+        rec = _batch_set(lengths, rho, u, T, steps, 50, pg, world, label)
+        if which == "specified":
+            out = rec
+            out["n_gpus"] = world
+            out["scaling"] = "strong (problems split across ranks)" if world > 1 else None
+            # training pairs written by the kernel itself, every 10 steps at every 16th node
+            with Batch(lengths, interp=8, tau=0.9) as b:
+                cap = 1 << 21
+                X = torch.empty((cap, 21), dtype=torch.float32, device="cuda")
+                Y = torch.empty((cap, 2), dtype=torch.float32, device="cuda")
+                b.set_state(rho, u, T)
+                b.set_pairs(X, Y, every=10, stride=16)
+                ms_pairs = replicas.max_over_ranks(pg, b.run(100, steps_per_launch=50))
+                pairs = b.pairs_written()
+            out["pairs"] = {"rows_per_100_steps": int(replicas.sum_over_ranks(pg, pairs)), "every": 10,
+                            "stride": 16, "ms_per_step_with_pairs": ms_pairs / 100}
+        else:
+            out["moderate_set"] = rec
+    return out
 
 
 def _time_steps(s, steps, warmup):
@@ -572,6 +721,230 @@ def run_configs(steps=5, warmup=2, d3q125_size=48):
     return out
 
 
+def _chunked(s, steps, chunk=50):
+    """Advance `steps` steps in calls of up to `chunk`; returns the summed
+    device time of the step kernels (CUDA events, ms)."""
+    ms = 0.0
+    for k0 in range(0, steps, chunk):
+        s.step(min(chunk, steps - k0))
+        ms += s.last_step_ms()
+    return ms
+
+
+def _drift(d0, d1, steps):
+    """Relative change of mass and energy over the run and per 1000 steps."""
+    m, e = (d1["mass"] - d0["mass"]) / d0["mass"], (d1["enrg"] - d0["enrg"]) / d0["enrg"]
+    return {"mass": m, "energy": e, "mass_per_1000_steps": m * 1000 / steps, "energy_per_1000_steps": e * 1000 / steps}
+
+
+def _l1_fields(a, b):
+    return {"rho": _l1(a["rho"], b["rho"]), "T": _l1(a["T"], b["T"])}
+
+
+def run_configs_full(which, d3q125_size=192, l1_size_d3q125=48):
+    """Full-length runs of the five configurations, one JSON object each
+    (keyed by configuration), every result with its L1 distance in rho and T
+    to this library's float64 path on the same run (itself held to the FP64
+    oracle by the GPU tests) and its relative mass and energy drift:
+
+      1  D1Q5 Sod, 1000 nodes, TVD, 500 steps, float64 (gamma 3, and gamma 1.4
+         with the energy populations): L1 to the exact Riemann solution; the
+         float32 path against the float64 one
+      2  D3Q27 Taylor-Green 128^3, quadratic, tau 0.51, 2000 steps, float32
+         against float64
+      3  the batched D1Q5 problems (the benchmark line's batch1d)
+      4  D3Q27 sphere 256^3, cubic, tau 0.52, 1500 steps: float32 plain and
+         learned (pairs from steps 121-150, the network attached from step 151)
+         against float64
+      5  D3Q125 shock + vortex at d3q125_size^3, WENO5 through the departure
+         point's row, inflow/outflow in x, 1000 steps, float32; L1 of float32
+         plain and learned against float64 at l1_size_d3q125^3 over the same
+         physical time; learned against plain speed at d3q125_size^3 after 200
+         steps.
+
+    Device time by CUDA events on the library's stream, summed over the
+    steps.  Progress goes to stderr."""
+    import torch
+
+    import lbmpond_b200 as pond
+    from lbmpond_b200.learned import Predictor, attach, calibrate_gate, collect_pairs, keep_history
+    from tests.riemann import sample
+    t_start = time.perf_counter()
+
+    def note(msg):
+        print(f"[configs-full {time.perf_counter() - t_start:7.1f} s] {msg}", file=sys.stderr, flush=True)
+
+    out = {}
+    if "1" in which:
+        n, lam2, nsteps = 1000, configs.SOD_LAMBDA2, 500
+        left, right = (1.0, 0.0, lam2 * 1.0), (0.125, 0.0, lam2 * 0.1 / 0.125)
+        x = (np.arange(n) - (n / 2 - 0.5)) / nsteps
+        for key, gamma, dof in (("sod_d1q5", 3.0, None), ("sod_d1q5_gamma14", 1.4, 4)):
+            res = {}
+            for prec in ("fp64", "fp32"):
+                with pond.Solver(lattice="D1Q5", shape=(n, 1, 1), precision=prec, interp=pond.TVD, tau=0.55,
+                                 bc=("clamp",) * 3, ddf_dof=dof) as s:
+                    s.init("sod", 0.5, *left, *right)
+                    d0 = s.diagnostics()
+                    ms = _chunked(s, nsteps)
+                    res[prec] = (s.fields(), _drift(d0, s.diagnostics(), nsteps), ms / nsteps)
+            er, eu, ep = sample((left[0], left[1], left[0] * left[2]), (right[0], right[1], right[0] * right[2]),
+                                gamma, x)
+            fr = res["fp64"][0]
+            out[key] = {"workload": f"D1Q5 Sod, {n} nodes, TVD, tau 0.55, zero-gradient ends, {nsteps} steps, gamma "
+                                    f"{gamma:g}" + (f" (energy populations, {dof} extra degrees of freedom)" if dof else ""),
+                        "fp64": {"ms_per_step": res["fp64"][2], "drift": res["fp64"][1],
+                                 "l1_vs_exact_riemann": {"rho": float(np.abs(fr["rho"] - er).mean() / er.mean()),
+                                                         "p": float(np.abs(fr["rho"] * fr["T"] - ep).mean() / ep.mean())}},
+                        "fp32": {"ms_per_step": res["fp32"][2], "drift": res["fp32"][1],
+                                 "l1_vs_fp64": _l1_fields(res["fp32"][0], fr)}}
+            note(f"{key} done")
+    if "2" in which:
+        n, nsteps = 128, 2000
+        res = {}
+        for prec in ("fp32", "fp64"):
+            with pond.Solver(lattice="D3Q27", shape=(n,) * 3, precision=prec, interp=pond.LAGR3, tau=0.51) as s:
+                s.init("tgv", *configs.tgv_params())
+                d0 = s.diagnostics()
+                ms, its, ks = 0.0, [], [d0["k"]]
+                for k0 in range(0, nsteps, 100):
+                    ms += _chunked(s, 100)
+                    d = s.diagnostics()
+                    its.append(d["niter_mean"])
+                    ks.append(d["k"])
+                res[prec] = (s.fields(), _drift(d0, d, nsteps), ms / nsteps, float(np.mean(its)), ks)
+            note(f"tgv {prec} done")
+        out["tgv_d3q27_128"] = {
+            "workload": f"D3Q27 Taylor-Green {n}^3, Mach 0.5, quadratic Lagrange, tau 0.51, {nsteps} steps",
+            "fp32": {"ms_per_step": res["fp32"][2], "MLUPS": n ** 3 / res["fp32"][2] / 1e3,
+                     "niter_mean": res["fp32"][3], "drift": res["fp32"][1],
+                     "l1_vs_fp64": _l1_fields(res["fp32"][0], res["fp64"][0]),
+                     "kinetic_energy_every_100_steps": res["fp32"][4]},
+            "fp64": {"ms_per_step": res["fp64"][2], "MLUPS": n ** 3 / res["fp64"][2] / 1e3,
+                     "niter_mean": res["fp64"][3], "drift": res["fp64"][1]}}
+    if "3" in which:
+        out["batch1d"] = run_batch1d(1000, 4096)
+        note("batch done")
+    if "4" in which:
+        n, nsteps, spin = 256, 1500, 150
+        mk = lambda prec="fp32": pond.Solver(lattice="D3Q27", shape=(n,) * 3, interp=pond.LAGR4,  # noqa: E731
+                                            precision=prec, tau=TAU, tol_abs=TOL_ABS if prec == "fp32" else None,
+                                            tol_rel=TOL_REL if prec == "fp32" else None)
+        res = {}
+        with mk("fp64") as s:
+            s.init("sphere", *sphere_params())
+            d0 = s.diagnostics()
+            ms = _chunked(s, nsteps)
+            res["fp64"] = (s.fields(), _drift(d0, s.diagnostics(), nsteps), ms / nsteps, s.diagnostics())
+        note("sphere fp64 done")
+        with mk() as s:
+            s.init("sphere", *sphere_params())
+            d0 = s.diagnostics()
+            ms = _chunked(s, nsteps)
+            d = s.diagnostics()
+            res["plain"] = (s.fields(), _drift(d0, d, nsteps), ms / nsteps, d)
+        note("sphere plain done")
+        cap = 4_000_000
+        X = torch.empty((cap, 39), dtype=torch.float32, device="cuda")
+        Y = torch.empty((cap, 4), dtype=torch.float32, device="cuda")
+        with mk() as s:
+            s.init("sphere", *sphere_params())
+            d0 = s.diagnostics()
+            rows = 0
+            ms = _chunked(s, spin - 30)
+            keep_history(s, True)
+            for k in range(30):
+                s.step(1)
+                ms += s.last_step_ms()
+                rows += collect_pairs(s, X, Y, offset_rows=rows, stride=61, seed=k)
+            keep_history(s, False)
+            net = Predictor(64, seed=0)
+            net.fit_stats(X[:rows], Y[:rows])
+            net.train(X[:rows], Y[:rows], steps=10000, batch=8192, lr=2e-3)
+            gate, _ = calibrate_gate(net, X[:rows], Y[:rows])
+            attach(s, net, gate=gate)
+            ms_l = _chunked(s, nsteps - spin)
+            d = s.diagnostics()
+            res["learned"] = (s.fields(), _drift(d0, d, nsteps), (ms + ms_l) / nsteps, d, ms_l / (nsteps - spin))
+            attach(s, None)
+            net.close()
+        note("sphere learned done")
+        fr = res["fp64"][0]
+        rec = {"workload": f"D3Q27 {n}^3 spherical Riemann problem, tau {TAU}, cubic Lagrange, {nsteps} steps",
+               "fp64": {"ms_per_step": res["fp64"][2], "drift": res["fp64"][1],
+                        "niter_mean_last_step": res["fp64"][3]["niter_mean"]}}
+        for key in ("plain", "learned"):
+            r = res[key]
+            rec[key] = {"ms_per_step": r[2], "MLUPS": n ** 3 / r[2] / 1e3, "drift": r[1],
+                        "niter_mean_last_step": r[3]["niter_mean"], "nonconverged_last_step": r[3]["nonconverged"],
+                        "l1_vs_fp64": _l1_fields(r[0], fr)}
+        rec["learned"]["ms_per_step_after_attach"] = res["learned"][4]
+        rec["learned"]["MLUPS_after_attach"] = n ** 3 / res["learned"][4] / 1e3
+        out["sphere_d3q27_256"] = rec
+    if "5" in which:
+        rec = {}
+        for label, m, nsteps in (("full", d3q125_size, 1000),
+                                 ("l1", l1_size_d3q125, max(1, round(1000 * l1_size_d3q125 / d3q125_size)))):
+            precs = ("fp32",) if label == "full" else ("fp32", "fp64")
+            fields = {}
+            for prec in precs:
+                with configs.build("shock_vortex_d3q125", size=m, precision=prec) as s:
+                    d0 = s.diagnostics()
+                    ms, its = 0.0, []
+                    for k0 in range(0, nsteps, 50):
+                        ms += _chunked(s, min(50, nsteps - k0))
+                        its.append(s.diagnostics()["niter_mean"])
+                    d = s.diagnostics()
+                    fields[prec] = s.fields()
+                    rec[f"{label}_{prec}"] = {"grid": f"{m}^3", "steps": nsteps, "ms_per_step": ms / nsteps,
+                                              "MLUPS": m ** 3 / (ms / nsteps) / 1e3, "niter_mean": float(np.mean(its)),
+                                              "niter_max_last_step": d["niter_max"],
+                                              "nonconverged_last_step": d["nonconverged"],
+                                              "drift": _drift(d0, d, nsteps)}
+                note(f"d3q125 {label} {prec} done")
+            if label == "l1":
+                rec["l1_fp32"]["l1_vs_fp64"] = _l1_fields(fields["fp32"], fields["fp64"])
+        # learned against plain at the full size, from the state after 200 steps
+        m = d3q125_size
+        with configs.build("shock_vortex_d3q125", size=m) as s, configs.build("shock_vortex_d3q125", size=m) as snap:
+            cap = 2_000_000
+            X = torch.zeros((cap, 39), dtype=torch.float32, device="cuda")
+            Y = torch.zeros((cap, 4), dtype=torch.float32, device="cuda")
+            s.step(180)
+            keep_history(s, True)
+            rows = 0
+            for k in range(20):
+                s.step(1)
+                rows += collect_pairs(s, X, Y, offset_rows=rows, stride=31, seed=k)
+            keep_history(s, False)
+            snap.copy_state_from(s)
+            ms_p = _chunked(s, 20, 20) / 20
+            dp = s.diagnostics()
+            fp = s.fields()
+            net = Predictor(128, seed=0)
+            net.fit_stats(X[:rows], Y[:rows])
+            loss = net.train(X[:rows], Y[:rows], steps=4000, batch=8192, lr=2e-3)
+            gate, _ = calibrate_gate(net, X[:rows], Y[:rows])
+            s.copy_state_from(snap)
+            attach(s, net, gate=gate)
+            ms_l = _chunked(s, 20, 20) / 20
+            dl = s.diagnostics()
+            fl = s.fields()
+            attach(s, None)
+            net.close()
+        rec["learned_vs_plain_after_200_steps"] = {
+            "grid": f"{m}^3", "steps": 20, "network": "39-128-128-4",
+            "plain": {"ms_per_step": ms_p, "MLUPS": m ** 3 / ms_p / 1e3, "niter_mean": dp["niter_mean"]},
+            "learned": {"ms_per_step": ms_l, "MLUPS": m ** 3 / ms_l / 1e3, "niter_mean": dl["niter_mean"],
+                        "pairs": rows, "loss_last": float(loss[-1]), "gate": gate},
+            "l1_learned_vs_plain": _l1_fields(fl, fp)}
+        note("d3q125 learned done")
+        rec["workload"] = ("D3Q125 Mach 1.5 shock + isentropic vortex, WENO5 (row through the departure point), "
+                           "inflow/outflow in x, periodic y/z, tau 0.9, float32")
+        out["shock_vortex_d3q125"] = rec
+    return out
+
+
 def run_mesh1d(steps=20, warmup=3, n=1 << 24):
     """The one-dimensional mesh path on a Sod tube of n nodes (float32, tau
     0.55, periodic): GAP2 on an AMR mask (every other node active, then one
@@ -634,9 +1007,13 @@ def run_reference(args, rank, world):
     blast as the timed GPU steps."""
     m = args.ref_size
     spin = round(args.spinup * m / 256)
-    v, dt, it, cores = _oracle_sample(m, spin, args.warmup, args.steps)
-    sample = (f"{m}^3 sample of the sphere problem after {spin} spin-up steps (the 256^3 spin-up scaled), "
-              f"FP64 oracle, {cores} threads, {it:.2f} iterations per node")
+    if os.path.exists(SAMPLE):
+        v, dt, it, it_gpu, cores, desc = _oracle_blocks(args.warmup, args.steps)
+        sample = f"{desc}; FP64 oracle, {cores} threads, {it:.2f} iterations per node"
+    else:
+        v, dt, it, cores = _oracle_sample(m, spin, args.warmup, args.steps)
+        sample = (f"{m}^3 sample of the sphere problem after {spin} spin-up steps (the 256^3 spin-up scaled), "
+                  f"FP64 oracle, {cores} threads, {it:.2f} iterations per node")
     return {"impl": "reference", "metric": METRIC, "value": v, "unit": "MLUPS", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -664,11 +1041,16 @@ def main():
     ap.add_argument("--ref-size", type=int, default=24)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--ref-cuda", action="store_true", help="with --impl reference: also time the reference's own kernels (64^3)")
+    ap.add_argument("--no-ref-cuda", dest="ref_cuda", action="store_false",
+                    help="skip the same-state comparison with the reference's own kernels (64^3 float64, 32^3 "
+                         "float32; the reference arm runs its kernels, this arm its own on the same runs)")
+    ap.add_argument("--gauge-tol", type=float, default=1e-8,
+                    help="also time the plain path with this absolute gauge tolerance (0: skip)")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched 1D measurement")
     ap.add_argument("--batch-steps", type=int, default=1000)
     ap.add_argument("--batch-problems", type=int, default=4096)
-    ap.add_argument("--workload", default="d3q27", choices=["d3q27", "batch1d", "configs", "mesh1d"],
+    ap.add_argument("--configs", default="12345", help="configs-full: which configurations (digits 1-5)")
+    ap.add_argument("--workload", default="d3q27", choices=["d3q27", "batch1d", "configs", "configs-full", "mesh1d"],
                     help="batch1d: only the batched D1Q5 measurement; configs: the other workloads (one JSON object); "
                          "mesh1d: the 1D mesh path (node mask, AMR, non-uniform positions)")
     ap.add_argument("--d3q125-size", type=int, default=48)
@@ -699,6 +1081,11 @@ def main():
         if int(os.environ.get("RANK", "0")) == 0:
             print(json.dumps(run_mesh1d(args.steps, args.warmup, args.mesh_size)), flush=True)
         return
+    if args.workload == "configs-full":
+        if int(os.environ.get("RANK", "0")) == 0:
+            for key, rec in run_configs_full(args.configs, args.d3q125_size).items():
+                print(json.dumps({key: rec}), flush=True)
+        return
     if args.workload == "configs":
         if int(os.environ.get("RANK", "0")) == 0:
             print(json.dumps(run_configs(args.steps, args.warmup, args.d3q125_size)), flush=True)
@@ -707,6 +1094,8 @@ def main():
     out = run_ours(args, rank, local, world, pg)
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(args.spinup)
+    if rank == 0 and world == 1 and args.ref_cuda:
+        out["same_state_as_reference_kernels"] = ours_same_state(local)
     if rank == 0 and world == 1 and not args.no_batch:
         out["batch1d"] = run_batch1d(args.batch_steps, args.batch_problems)
     if pg is not None:

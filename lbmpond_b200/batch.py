@@ -41,6 +41,26 @@ def riemann_problems(nproblems=4096, seed=0, lmin=256, lmax=4096):
     return lengths, rho, u, T
 
 
+def riemann_problems_moderate(nproblems=4096, seed=0, lmin=256, lmax=4096, lam=0.3, rho_ratio=10.0, T_ratio=2.0,
+                              u_scale=0.3):
+    """A well-posed companion of riemann_problems: per side rho log-uniform
+    with a ratio of at most `rho_ratio` across the jump, temperature
+    log-uniform with a ratio of at most `T_ratio`, in lattice units
+    T = lam^2 * T_phys with T_phys around 1, and u uniform in
+    lam * u_scale * [-1, 1].  The specified set (ratios up to 100 in rho and
+    in p, independently) drives the reference iteration non-finite on most
+    problems; on this set the float64 oracle keeps every sampled problem
+    finite."""
+    rng = np.random.default_rng(seed)
+    lengths = rng.integers(lmin, lmax + 1, nproblems).astype(np.int32)
+    rho_lr = np.exp(rng.uniform(-0.5 * np.log(rho_ratio), 0.5 * np.log(rho_ratio), (nproblems, 2)))
+    T_lr = lam ** 2 * np.exp(rng.uniform(-0.5 * np.log(T_ratio), 0.5 * np.log(T_ratio), (nproblems, 2)))
+    u_lr = lam * u_scale * rng.uniform(-1.0, 1.0, (nproblems, 2))
+    side = np.concatenate([(np.arange(n) >= n // 2).astype(np.int64) for n in lengths])
+    prob = np.repeat(np.arange(nproblems), lengths)
+    return lengths, rho_lr[prob, side], u_lr[prob, side], T_lr[prob, side]
+
+
 class Batch:
     """A set of independent D1Q5 problems stepped together on one GPU."""
 

@@ -16,8 +16,9 @@
 //
 // State file (little endian): int32 magic 0x504f4e44, int32 Q, int64 nx, ny,
 // nz, then float64 f[Q*N], rho[N], g[4*N] (u_x,u_y,u_z,T), x fastest.  The
-// output file appends int32 NiterMax of the last step, int32 nsteps and
-// float32 kernel milliseconds per step.
+// output file appends int32 NiterMax of the last step, int32 nsteps,
+// float32 kernel milliseconds per step and the float64 mean of the last
+// step's per-node iteration counts.
 //
 // Mesh mode (the 1D adaptive-mesh code the reference's calcStep leaves
 // commented, enabled by build_ref.sh's gap2 / nu3 schemes): <in.mesh> holds
@@ -272,6 +273,14 @@ int main(int argc, char** argv) {
   fwrite(f.data(), 8, f.size(), fp); fwrite(rho.data(), 8, rho.size(), fp); fwrite(g.data(), 8, g.size(), fp);
   const int32_t ns = nsteps;
   fwrite(&niter_max, 4, 1, fp); fwrite(&ns, 4, 1, fp); fwrite(ms.data(), 4, ms.size(), fp);
+  {  // mean of the per-node iteration counts of the last step (Cinfo::niter, steps.cu:417,508)
+    std::vector<Cinfo> ci(N);
+    CHECK_ERROR(cudaMemcpy(ci.data(), parsHost.cinfo, N * sizeof(Cinfo), cudaMemcpyDeviceToHost));
+    double sum = 0;
+    for (int64_t i = 0; i < N; i++) sum += ci[i].niter;
+    const double mean = N ? sum / double(N) : 0.0;
+    fwrite(&mean, 8, 1, fp);
+  }
   fclose(fp);
   printf("ref_pond: Q=%d %ldx%ldx%ld steps=%d NiterMax=%d ms/step(last)=%.3f\n", Qn, (long)n[0], (long)n[1],
          (long)n[2], nsteps, niter_max, ms.empty() ? 0.f : ms.back());

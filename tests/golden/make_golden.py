@@ -64,6 +64,20 @@ def read_state(path, Q, shape):
     return f, rho, g, niter_max, ms
 
 
+def read_niter_mean(path, Q, shape):
+    """The mean per-node iteration count of the last step, appended after the
+    state by oracle/ref_main.cu (None for an output without it)."""
+    N = int(np.prod(shape))
+    skip = 8 + 24 + 8 * (Q + 5) * N
+    with open(path, "rb") as fp:
+        fp.seek(skip)
+        fp.read(4)
+        ns = int(np.fromfile(fp, dtype=np.int32, count=1)[0])
+        fp.seek(4 * ns, 1)
+        tail = np.fromfile(fp, dtype=np.float64, count=1)
+    return float(tail[0]) if tail.size else None
+
+
 MESH_MAGIC = 0x4D455348
 
 
