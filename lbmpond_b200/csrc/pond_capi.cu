@@ -677,7 +677,6 @@ int pond_copy_state(pond_ctx* dst, pond_ctx* src) {
     if (e == cudaSuccess) e = cudaStreamSynchronize(dst->stream);
     if (e != cudaSuccess) return cuda_fail(e, "pond_copy_state");
     dst->n_active = src->n_active;
-    dst->part_dirty = true;
   }
   dst->initialized = true;
   dst->have_sums = false;

@@ -184,10 +184,6 @@ template <typename R> struct StepArgs {
   // one-dimensional mesh schemes: node mask (nonzero = active) and node positions, or null
   const uint8_t* mask = nullptr;  // [N]
   const double* pos = nullptr;    // [N]
-  // the nodes partitioned into the active ones and then the inactive ones,
-  // each in node order (thread t of the mesh kernels takes node part[t]), or null
-  const int* part = nullptr;      // [N]
-  long long n_active = 0;
   // state of the inflow ghost node of POND_BC_INFLOW axes: rho, u_x, u_y, u_z, T
   double inflow[5] = {1, 0, 0, 0, 1};
 };

@@ -48,10 +48,6 @@ struct pond_ctx {
   int mask_cur = 0;
   long long n_active = 0;                 // active nodes in mask[mask_cur]
   double* pos = nullptr;                  // node positions (POND_NONUNIFORM3)
-  int* part = nullptr;                    // nodes, active ones first, each part in node order [N]
-  int* part_counts = nullptr;             // active nodes per block of the partition
-  int* part_offs = nullptr;               // their exclusive prefix (+ the total at the end)
-  bool part_dirty = true;                 // the mask changed since the partition was built
   uint8_t* amr_code = nullptr;            // coarsening: per-node transition codes [N]
   uint32_t* amr_maps = nullptr;           // coarsening: per-chunk composed transitions
   uint8_t* amr_sigma = nullptr;           // coarsening: automaton state entering each chunk
@@ -98,8 +94,6 @@ int mesh_alloc(pond_ctx* c);
 // every node active, positions p_x = x (fill, init.cu:100-106)
 int mesh_reset(pond_ctx* c);
 void mesh_free(pond_ctx* c);
-// rebuild the active/inactive partition of the nodes if the mask changed
-int mesh_partition(pond_ctx* c);
 // the adaptation policy after one step: rescale the new state when NiterMax crosses a threshold
 int dt_adapt_after_step(pond_ctx* c);
 }  // namespace pond

@@ -42,83 +42,6 @@ __global__ void init_kernel(uint8_t* mask, double* pos, long long n) {
   }
 }
 
-// ---------------------------------------------------------------- partition
-// The nodes split into the active ones and then the inactive ones, each in
-// node order: per block of PB nodes an active count, one block's exclusive
-// scan of the counts, and a stable write (warp ballots).  An active node x
-// goes to slot (actives before x), an inactive one to
-// n_active + x - (actives before x).
-constexpr int PB = 1024, PT = 256;  // nodes per partition block, its threads
-
-__global__ void __launch_bounds__(PT) part_count_kernel(const uint8_t* mask, int n, int* counts) {
-  __shared__ int ws[PT / 32];
-  const int base = blockIdx.x * PB;
-  int c = 0;
-#pragma unroll
-  for (int j = 0; j < PB / PT; j++) {
-    const int x = base + j * PT + threadIdx.x;
-    c += (x < n && mask[x]) ? 1 : 0;
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = c;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int t = 0;
-    for (int w = 0; w < PT / 32; w++) t += ws[w];
-    counts[blockIdx.x] = t;
-  }
-}
-
-// one block of SCAN_THREADS: offs[b] = sum of counts[0..b-1]; offs[nb] = total
-__global__ void __launch_bounds__(SCAN_THREADS) part_scan_kernel(const int* counts, int nb, int* offs) {
-  __shared__ int sm[SCAN_THREADS];
-  const int t = threadIdx.x;
-  const int per = (nb + SCAN_THREADS - 1) / SCAN_THREADS;
-  const int b0 = min(t * per, nb), b1 = min(b0 + per, nb);
-  int run = 0;
-  for (int b = b0; b < b1; b++) run += counts[b];
-  sm[t] = run;
-  __syncthreads();
-  for (int off = 1; off < SCAN_THREADS; off <<= 1) {
-    const int v = t >= off ? sm[t - off] : 0;
-    __syncthreads();
-    sm[t] += v;
-    __syncthreads();
-  }
-  int acc = t == 0 ? 0 : sm[t - 1];
-  for (int b = b0; b < b1; b++) {
-    offs[b] = acc;
-    acc += counts[b];
-  }
-  if (t == SCAN_THREADS - 1) offs[nb] = sm[t];
-}
-
-__global__ void __launch_bounds__(PT) part_write_kernel(const uint8_t* mask, int n, const int* offs, int nb,
-                                                         int* part) {
-  __shared__ int ws[PT / 32];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int total = offs[nb];
-  int before = offs[blockIdx.x];  // actives ahead of this round
-  const int base = blockIdx.x * PB;
-  for (int j = 0; j < PB / PT; j++) {
-    const int x = base + j * PT + threadIdx.x;
-    const bool a = x < n && mask[x];
-    const unsigned bal = __ballot_sync(0xffffffffu, a);
-    if (lane == 0) ws[warp] = __popc(bal);
-    __syncthreads();
-    int ahead = before + __popc(bal & ((1u << lane) - 1u));
-    int round = 0;
-    for (int w = 0; w < PT / 32; w++) {
-      if (w < warp) ahead += ws[w];
-      round += ws[w];
-    }
-    if (x < n) part[a ? ahead : total + (x - ahead)] = x;
-    before += round;
-    __syncthreads();
-  }
-}
-
 // ---------------------------------------------------------------- refinement
 // AMR_add (amr.cu:1-27): reads the old mask `set`, activates midpoints in
 // `setnew` (a copy of it).  Each thread's reads are of active nodes and its
@@ -363,10 +286,8 @@ template <typename R> __global__ void rescale_kernel(R* g, long long N, double s
 
 int mesh_alloc(pond_ctx* c) {
   if (!mesh_scheme(c->p.interp)) return POND_OK;
-  const size_t N = (size_t)c->N, nb = (N + mesh::PB - 1) / mesh::PB;
+  const size_t N = (size_t)c->N;
   if (cudaMalloc(&c->mask[0], N) != cudaSuccess || cudaMalloc(&c->mask[1], N) != cudaSuccess ||
-      cudaMalloc(&c->part, N * sizeof(int)) != cudaSuccess || cudaMalloc(&c->part_counts, nb * sizeof(int)) != cudaSuccess ||
-      cudaMalloc(&c->part_offs, (nb + 1) * sizeof(int)) != cudaSuccess ||
       (c->p.interp == POND_NONUNIFORM3 && cudaMalloc(&c->pos, N * sizeof(double)) != cudaSuccess)) {
     cudaGetLastError();
     return set_error(POND_ERR_NOMEM, "node mask / positions");
@@ -384,28 +305,11 @@ int mesh_reset(pond_ctx* c) {
   if (e != cudaSuccess) return cuda_fail(e, "mesh init");
   c->mask_cur = 0;
   c->n_active = c->N;
-  c->part_dirty = true;
-  return POND_OK;
-}
-
-int mesh_partition(pond_ctx* c) {
-  if (!c->part_dirty) return POND_OK;
-  const int n = (int)c->N;
-  const int nb = (n + mesh::PB - 1) / mesh::PB;
-  const uint8_t* m = c->mask[c->mask_cur];
-  mesh::part_count_kernel<<<nb, mesh::PT, 0, c->stream>>>(m, n, c->part_counts);
-  mesh::part_scan_kernel<<<1, mesh::SCAN_THREADS, 0, c->stream>>>(c->part_counts, nb, c->part_offs);
-  mesh::part_write_kernel<<<nb, mesh::PT, 0, c->stream>>>(m, n, c->part_offs, nb, c->part);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return cuda_fail(e, "partition kernel launch");
-  c->part_dirty = false;
   return POND_OK;
 }
 
 void mesh_free(pond_ctx* c) {
   cudaFree(c->mask[0]); cudaFree(c->mask[1]); cudaFree(c->pos);
-  cudaFree(c->part); cudaFree(c->part_counts); cudaFree(c->part_offs);
-  c->part = c->part_counts = c->part_offs = nullptr;
   cudaFree(c->amr_code); cudaFree(c->amr_maps); cudaFree(c->amr_sigma); cudaFree(c->amr_counts);
   if (c->amr_counts_h) cudaFreeHost(c->amr_counts_h);
   c->mask[0] = c->mask[1] = nullptr;
@@ -520,7 +424,6 @@ int pond_set_mask(pond_ctx* c, const uint8_t* mask) {
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_fail(e, "pond_set_mask");
   c->n_active = active;
-  c->part_dirty = true;
   return POND_OK;
 }
 
@@ -571,7 +474,6 @@ int pond_amr_refine(pond_ctx* c, double tol, int64_t* added, int64_t* limit_hits
   if (st == POND_OK) st = c->elem == 8 ? refine_typed<double>(c, tol) : refine_typed<float>(c, tol);
   if (st != POND_OK) return st;
   c->mask_cur = 1 - c->mask_cur;
-  c->part_dirty = true;
   c->n_active += (long long)c->amr_counts_h[0];
   if (added) *added = (int64_t)c->amr_counts_h[0];
   if (limit_hits) *limit_hits = (int64_t)c->amr_counts_h[1];
@@ -602,7 +504,6 @@ int pond_amr_coarsen(pond_ctx* c, double tol, int64_t* removed) {
   st = c->elem == 8 ? coarsen_typed<double>(c, tol) : coarsen_typed<float>(c, tol);
   if (st != POND_OK) return st;
   c->mask_cur = 1 - c->mask_cur;
-  c->part_dirty = true;
   c->n_active -= (long long)c->amr_counts_h[0];
   if (removed) *removed = (int64_t)c->amr_counts_h[0];
   return POND_OK;

@@ -212,12 +212,6 @@ template <typename R> static int launch_typed(pond_ctx* c, const void* const* in
     if (c->p.bc[k] == POND_BC_INFLOW && !c->have_inflow)
       return set_error(POND_ERR_STATE, "an inflow boundary needs pond_set_inflow before stepping");
   for (int k = 0; k < 5; k++) a.inflow[k] = c->inflow[k];
-  if (c->mask[0]) {
-    const int pst = mesh_partition(c);
-    if (pst != POND_OK) return pst;
-    a.part = c->part;
-    a.n_active = c->n_active;
-  }
   cudaError_t e = cudaMemsetAsync(c->d_sums, 0, sizeof(StepSums), c->stream);
   if (e != cudaSuccess) return cuda_fail(e, "memset sums");
   cudaStream_t s = c->stream;

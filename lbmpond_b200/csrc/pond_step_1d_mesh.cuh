@@ -13,10 +13,13 @@
 //
 // An inactive node is skipped by the reference's step (steps.cu:359) and left
 // unwritten; here it is carried over unchanged so that the output buffer is
-// always a complete state.  Threads take their nodes from a partition of the
-// grid (the active nodes, then the inactive ones, each in node order), so a
-// warp either steps 32 active nodes or copies 32 inactive ones whatever the
-// mask's pattern.  The gauge iteration, moments, convergence test and BGK are
+// always a complete state.  Each CTA takes a window of 128 consecutive nodes
+// and hands its threads the window's active nodes first and then its inactive
+// ones (each in node order), so a warp mostly either steps active nodes or
+// copies inactive ones whatever the mask's pattern, and both halves of every
+// 32-byte sector of the output are written by one CTA within microseconds
+// (an L2 line that two far-apart launches half-write costs DRAM read-modify-
+// write traffic).  The gauge iteration, moments, convergence test and BGK are
 // those of the other kernels (moments_and_test / finish_node); the
 // conservation sums cover active nodes, weighted under NONUNIFORM3 by half
 // the distance between the node's neighbours (update.cu:52-69).
@@ -64,17 +67,32 @@ template <int SCHEME, typename R>
 __global__ void __launch_bounds__(128) pull_1d_mesh_kernel(StepArgs<R> a) {
   using L = Lattice<POND_D1Q5>;
   constexpr int Q = 5;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  int x = t;
+  // the window's nodes, active ones first (stable), then inactive ones
+  __shared__ int wnode[128];
+  __shared__ int wcount[2][4];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int x = blockIdx.x * 128 + threadIdx.x;
   bool act = false;
-  if (t < a.nx) {
-    if (a.part) {
-      x = a.part[t];
-      act = t < a.n_active;
-    } else {
-      act = mesh_active(a.mask, x);
+  {
+    const bool mine = x < a.nx;
+    const bool a_me = mine && mesh_active(a.mask, x);
+    const unsigned ba = __ballot_sync(0xffffffffu, a_me), bi = __ballot_sync(0xffffffffu, mine && !a_me);
+    if (lane == 0) { wcount[0][warp] = __popc(ba); wcount[1][warp] = __popc(bi); }
+    __syncthreads();
+    int na = 0, ni = 0, pa = 0, pi = 0;
+#pragma unroll
+    for (int w = 0; w < 4; w++) {
+      if (w < warp) { pa += wcount[0][w]; pi += wcount[1][w]; }
+      na += wcount[0][w]; ni += wcount[1][w];
     }
+    const unsigned below = (1u << lane) - 1u;
+    if (a_me) wnode[pa + __popc(ba & below)] = x;
+    else if (mine) wnode[na + pi + __popc(bi & below)] = x;
+    __syncthreads();
+    act = (int)threadIdx.x < na;
+    x = (int)threadIdx.x < na + ni ? wnode[threadIdx.x] : a.nx;
   }
+  const int t = x;
   NodeSums ns = {0, 0, 0, 0, 0, 0, 0ull, 0ull, 0ull, 0};
   if (t < a.nx && !act) {
 #pragma unroll
