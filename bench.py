@@ -331,6 +331,20 @@ def run_ours(args, rank, local, world, pg):
              "iterations_mean": p1["niter_mean"], "iterations_max": p1["niter_max"],
              "nonconverged": p1["nonconverged"]}
 
+    # iterations per node of one more plain step, and what a perfect starting
+    # gauge could save: the first convergence test compares the new
+    # populations with the previous time level's (steps.cu:360-510), so a node
+    # whose populations change needs two iterations whatever its start and an
+    # unchanged node one
+    s.keep_niter(True)
+    s.step(1)
+    ni = s.niter()
+    s.keep_niter(False)
+    hist = np.bincount(np.minimum(ni, 12), minlength=13)[1:].tolist()
+    ceiling = {"histogram_1_to_12plus": hist, "plain_mean": float(ni.mean()),
+               "perfect_start_mean": float(np.minimum(ni, 2).mean()),
+               "iteration_ratio": float(ni.mean() / np.minimum(ni, 2).mean())}
+
     # the same plain path with the convergence test of u and T at an absolute
     # 1e-8 (float64 gauge residual), the populations' test at the float32 floor
     gauge_tight = None
@@ -478,6 +492,7 @@ def run_ours(args, rank, local, world, pg):
                    "timed_steps": f"{args.spinup + args.warmup + 1}..{args.spinup + args.warmup + args.steps}"},
         "plain": plain, "learned": learned, "plain_gauge_residual_1e8": gauge_tight,
         "speedup_learned_vs_plain": (learned["value"] / plain["value"]) if learned else None,
+        "learned_start_ceiling": ceiling,
         "l1_vs_fp64": l1, "drift": drift,
         "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved_gbs / hbm_peak, "traffic": traffic, "peak_source": "measured",
