@@ -58,9 +58,11 @@ enum {
                            steps.cu:1122-1149 (call site :449) */
   POND_NONUNIFORM3 = 10, /* quadratic Lagrange on the node positions of x-1, x, x+1,
                            propagateNR_1D + LagrPolNR_1D, steps.cu:882-908,590-594 (call site :453) */
-  /* WENO5 whose smoothness indicators read the row through the departure
-     point (y = floor(crd.y+0.5), z = floor(crd.z+0.5)) instead of the
-     reference's y = z = floor(crd.x+0.5); the same as POND_WENO5 on 1D grids */
+  /* centred WENO5: the candidates' y and z windows centred on the departure
+     point (nodes floor(c+0.5)-1 .. floor(c+0.5)+1; the reference's start at
+     floor(c+0.5) and extrapolate, steps.cu:776-778) and the smoothness row
+     through it (y = floor(crd.y+0.5), z = floor(crd.z+0.5) instead of the
+     reference's y = z = floor(crd.x+0.5)); the same as POND_WENO5 on 1D grids */
   POND_WENO5_ROW = 11
 };
 /* boundaries per axis: periodic is the reference (steps.cu:1015-1017); mirror

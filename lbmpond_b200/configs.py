@@ -135,7 +135,7 @@ PRESETS = {
         lambda s, n: s.init("sphere", *sphere_params()), 1500),
     "shock_vortex_d3q125": Preset(
         "D3Q125 Mach 1.5 normal shock at x = 0.5 + isentropic vortex (strength 0.3, radius 0.05) at (0.25, 0.5), "
-        "WENO5 (smoothness row through the departure point), tau 0.9, inflow of the pre-shock state below x = 0 "
+        "centred WENO5 (POND_WENO5_ROW), tau 0.9, inflow of the pre-shock state below x = 0 "
         "and zero-gradient outflow above x = 1, periodic y and z, float32",
         192, lambda n: dict(lattice="D3Q125", shape=(n, n, n), precision="fp32", tau=0.9, interp=11,
                             bc=("inflow", "periodic", "periodic")), _shock_vortex_init(5.0 / 3.0), 1000),

@@ -1,18 +1,18 @@
-// D3Q125 PonD pull step with WENO5 interpolation whose smoothness indicators
-// read the row through the departure point (POND_WENO5_ROW), float32: a tile
-// of nodes per CTA, a warp per node at a time.
+// D3Q125 PonD pull step with the centred WENO5 (POND_WENO5_ROW), float32: a
+// tile of nodes per CTA, a warp per node at a time.
 //
-// The arithmetic is pull_weno3d_kernel's (propagateWENO<3,5>, steps.cu:774-825):
-// three quadratic candidates on x nodes fx-2+s .. fx+s, y nodes fy .. fy+2
-// and z nodes fz .. fz+2 (fx = floor(crd.x+0.5), likewise fy, fz), blended
-// with Jiang-Shu weights from five transferred values on the row
+// The arithmetic is pull_weno3d_kernel's centred variant (propagateWENO<3,5>,
+// steps.cu:774-825, with the y/z windows centred): three quadratic
+// candidates on x nodes fx-2+s .. fx+s, y nodes fy-1 .. fy+1 and z nodes
+// fz-1 .. fz+1 (fx = floor(crd.x+0.5), likewise fy, fz), blended with
+// Jiang-Shu weights from five transferred values on the row
 // (fx-2 .. fx+2, fy, fz).  Organised for the SM like the fixed-stencil
 // D3Q125 tile kernel:
 //
 //  * a CTA owns a 4 x 2 x 2 tile and stages it once per step with the halo
 //    the windows reach while |v| < 1.5 along every axis: 3 nodes on both
-//    sides in x, 1 below and 3 above in y and z (10 x 6 x 6 nodes, 125
-//    population planes and the gauge, 186 KB);
+//    sides in x, 2 in y and z (10 x 6 x 6 nodes, 125 population planes and
+//    the gauge, 186 KB);
 //  * every staged node is transferred into the tile's reference gauge R
 //    once (three passes of the 5x5 basis); the transfer of a source node into
 //    a target gauge equals R -> target applied to its R-gauge populations,
@@ -26,7 +26,7 @@
 //    every target y-class (a per-warp table); per stencil row it gathers the
 //    five R x-classes of its column by shuffle, applies its target x-class
 //    transfer and adds the row into the three candidate sums.  The
-//    smoothness row is the same contraction with unit weights on the first
+//    smoothness row is the same contraction with unit weights on the middle
 //    window node in y and z;
 //  * a warp whose node's windows leave the staged halo runs that iteration
 //    from global memory (the group transfer of pull_weno3d_kernel).
@@ -38,7 +38,7 @@ namespace pond {
 namespace d125w {
 
 constexpr int TX = 4, TY = 2, TZ = 2;      // tile
-constexpr int HXL = 3, HXH = 3, HL = 1, HH = 3;  // halo: x both sides; y and z below / above
+constexpr int HXL = 3, HXH = 3, HL = 2, HH = 2;  // halo: x both sides; y and z below / above
 constexpr int SX = TX + HXL + HXH, SY = TY + HL + HH, SZ = TZ + HL + HH;
 constexpr int SN = SX * SY * SZ;  // 360 staged nodes
 constexpr int PS = SN + 1;        // plane stride: odd, so the five R x-classes of a load hit distinct banks
@@ -51,7 +51,7 @@ struct Smem {
   float u[3][SN];             // staged velocities (sign-flipped on mirrored axes)
   float c[SN];                // sqrts(T / TLat)
   unsigned char flags[SN];    // mirrored axes (bits 0-2)
-  float GY[WARPS][5][25];     // per warp: y weight x transfer entry, [oy + 1][5 i2 + k2]
+  float GY[WARPS][5][25];     // per warp: y weight x transfer entry, [oy + HL][5 i2 + k2]
   float GD[WARPS][25];        // per warp: the y transfer itself, [5 i2 + k2]
 };
 static_assert(sizeof(Smem) + 4096 <= 232448, "the tile must fit one CTA");
@@ -212,7 +212,7 @@ __global__ void __launch_bounds__(THREADS, 1) pull_d3q125_weno_tile_kernel(StepA
 #pragma unroll
         for (int s = 0; s < 3; s++) lagr_weights<3, R>(crdx - (fxd - 2 + s), LX[s]);
         const double crdz = double(z) - (C * L::xi1(k) + U[2]);
-        const double fzd = floor(crdz + 0.5);
+        const double fzd = floor(crdz + 0.5) - 1;  // centred window: fz-1 .. fz+1
         const int bz = w3d::clamp_off((int)fzd - z);
         R WZ[3];
         lagr_weights<3, R>(crdz - fzd, WZ);
@@ -221,7 +221,7 @@ __global__ void __launch_bounds__(THREADS, 1) pull_d3q125_weno_tile_kernel(StepA
 #pragma unroll
         for (int i2 = 0; i2 < 5; i2++) {
           const double crdy = double(y) - (C * L::xi1(i2) + U[1]);
-          const double fyd = floor(crdy + 0.5);
+          const double fyd = floor(crdy + 0.5) - 1;
           by[i2] = w3d::clamp_off((int)fyd - y);
           lagr_weights<3, R>(crdy - fyd, WY[i2]);
         }
@@ -296,7 +296,7 @@ __global__ void __launch_bounds__(THREADS, 1) pull_d3q125_weno_tile_kernel(StepA
 #pragma unroll
                   for (int k3 = 0; k3 < 5; k3++) zr = fmaf(tz[k3], fq[(5 * k2 + k3) * PS], zr);
                   Zc[k2] = fmaf(wz, zr, Zc[k2]);
-                  Zd[k2] = jz == 0 ? zr : Zd[k2];
+                  Zd[k2] = jz == 1 ? zr : Zd[k2];
                 }
               }
               const R* gy = sm.GY[warp][oy + HL];
@@ -310,7 +310,7 @@ __global__ void __launch_bounds__(THREADS, 1) pull_d3q125_weno_tile_kernel(StepA
                   td = fmaf(gd[5 * i2 + k2], Zd[k2], td);
                 }
                 Yr[i2] = t;
-                Yd[i2] = oy == by[i2] ? td : Yd[i2];
+                Yd[i2] = oy == by[i2] + 1 ? td : Yd[i2];
               }
             }
             // the row: gather the five R x-classes of this lane's column

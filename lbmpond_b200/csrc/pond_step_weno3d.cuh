@@ -7,9 +7,12 @@
 // likewise fy, fz (:776-778, the y/z windows start at the rounded
 // coordinate), and blends them with Jiang-Shu weights from the smoothness
 // indicators of five transferred values on one x-row (:780-815).  The
-// reference reads that row at y = z = floor(crd.x+0.5) (:783); POND_WENO5
-// keeps this, POND_WENO5_ROW reads the row through the departure point
-// (y = fy, z = fz) instead.  On 1D grids both are row 0.
+// reference reads that row at y = z = floor(crd.x+0.5) (:783), and its y/z
+// windows start at the rounded coordinate, so the quadratic extrapolates
+// (weights up to 1.875, -1.25, 0.375); POND_WENO5 keeps both.  POND_WENO5_ROW
+// centres the y/z windows on the rounded coordinate (fy-1 .. fy+1) and reads
+// the smoothness row through the departure point (y = fy, z = fz).  On 1D
+// grids both are the same.
 //
 // Organisation: a group of Q1*Q1 lanes steps one node (D3Q125: 25 lanes, one
 // node per warp; D3Q27: 9 lanes, three nodes per warp).  Lane (p, k) owns the
@@ -176,8 +179,9 @@ __device__ __forceinline__ int clamp_off(int o) { return o < -MAXOFF ? -MAXOFF :
 // 32 lanes call it together; `done` lanes contribute no window.  Windows
 // (relative offsets): x nodes bx .. bx+4 with candidate s on bx+s .. bx+s+2
 // (weights LX[s]), z nodes bz .. bz+2 (WZ), y nodes by[i2] .. by[i2]+2
-// (WY[i2]).  `work` counts the sites transferred (leader lane only).
-template <int LAT, typename R, bool kRowFix>
+// (WY[i2]); the centred variant's smoothness row is the middle node of the
+// y and z windows.  `work` counts the sites transferred (leader lane only).
+template <int LAT, typename R, bool kCentred>
 __device__ __forceinline__ void accumulate_global(const StepArgs<R>& a, int x, int y, int z, bool done, int base,
                                                   int p, int k, const R Uc[3], R invC, int bx, const R LX[3][3],
                                                   int bz, const R WZ[3], const int by[Lattice<LAT>::Q1],
@@ -225,7 +229,7 @@ __device__ __forceinline__ void accumulate_global(const StepArgs<R>& a, int x, i
           const R v = wy * wz * fT[i2];
 #pragma unroll
           for (int s = 0; s < 3; s++) S[s][i2] = fma(lxs[s], v, S[s][i2]);
-          if (kRowFix && jy == 0 && jz == 0) {
+          if (kCentred && jy == 1 && jz == 1) {
 #pragma unroll
             for (int m = 0; m < 5; m++) U5[m][i2] = (jx == m) ? fT[i2] : U5[m][i2];
           }
@@ -233,7 +237,7 @@ __device__ __forceinline__ void accumulate_global(const StepArgs<R>& a, int x, i
       }
     }
   }
-  if (!kRowFix) {
+  if (!kCentred) {
     // the reference's smoothness row (:783): nodes fx-2 .. fx+2 at y = z = fx
     // (absolute coordinates; fx = x + bx + 2 for this lane's x-class)
     const int fl = __reduce_min_sync(0xffffffffu, done ? MAXOFF : bx + 2);
@@ -257,8 +261,9 @@ __device__ __forceinline__ void accumulate_global(const StepArgs<R>& a, int x, i
   }
 }
 
-// The WENO5 step.  kRowFix: smoothness row through the departure point.
-template <int LAT, typename R, bool kRowFix>
+// The WENO5 step.  kCentred: y/z windows centred and the smoothness row
+// through the departure point (POND_WENO5_ROW).
+template <int LAT, typename R, bool kCentred>
 __global__ void __launch_bounds__(THREADS) pull_weno3d_kernel(StepArgs<R> a) {
   using L = Lattice<LAT>;
   constexpr int Q1 = L::Q1, G = Geo<LAT>::G, NPW = Geo<LAT>::NPW;
@@ -310,8 +315,10 @@ __global__ void __launch_bounds__(THREADS) pull_weno3d_kernel(StepArgs<R> a) {
     R LX[3][3];                                   // candidate s on nodes bx+s .. bx+s+2
 #pragma unroll
     for (int s = 0; s < 3; s++) lagr_weights<3, R>(crdx - (fxd - 2 + s), LX[s]);
+    // y/z windows from floor(c+0.5) (the reference) or floor(c+0.5)-1 (centred)
+    constexpr int yz0 = kCentred ? 1 : 0;
     const double crdz = double(z) - (C * L::xi1(k) + U[2]);
-    const double fzd = floor(crdz + 0.5);
+    const double fzd = floor(crdz + 0.5) - yz0;
     const int bz = clamp_off((int)fzd - z);
     R WZ[3];
     lagr_weights<3, R>(crdz - fzd, WZ);
@@ -320,12 +327,12 @@ __global__ void __launch_bounds__(THREADS) pull_weno3d_kernel(StepArgs<R> a) {
 #pragma unroll
     for (int i2 = 0; i2 < Q1; i2++) {
       const double crdy = double(y) - (C * L::xi1(i2) + U[1]);
-      const double fyd = floor(crdy + 0.5);
+      const double fyd = floor(crdy + 0.5) - yz0;
       by[i2] = clamp_off((int)fyd - y);
       lagr_weights<3, R>(crdy - fyd, WY[i2]);
     }
     R S[3][Q1], U5[5][Q1];
-    accumulate_global<LAT, R, kRowFix>(a, x, y, z, done, base, p, k, Uc, invC, bx, LX, bz, WZ, by, WY, S, U5, work,
+    accumulate_global<LAT, R, kCentred>(a, x, y, z, done, base, p, k, Uc, invC, bx, LX, bz, WZ, by, WY, S, U5, work,
                                        lane == base);
     // blend, calcMoments (structs.cuh:315-342) and isConv (steps.cu:58-75) in float64
     R acc[Q1];

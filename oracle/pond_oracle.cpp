@@ -428,17 +428,21 @@ double lagr_eval(const Domain& D, int N, const double crd[3], const int64_t cl[3
   return fpr;
 }
 
-// steps.cu:774-825 propagateWENO<3,5>.  row_fix: the smoothness indicators
-// read the row through the departure point (y = floor(crd.y+0.5), z =
-// floor(crd.z+0.5), the first row of the three sub-stencils) instead of the
-// reference's y = z = floor(crd.x+0.5) (:783), which in 3D lies elsewhere in
-// the domain; on 1D grids both are row 0.
+// steps.cu:774-825 propagateWENO<3,5>.  centred: the variant with the
+// candidates' y and z windows centred on the departure point (nodes
+// floor(c+0.5)-1 .. floor(c+0.5)+1 instead of the reference's floor(c+0.5) ..
+// floor(c+0.5)+2, :776-778, which extrapolate) and the smoothness indicators
+// read on the row through the departure point (y = floor(crd.y+0.5), z =
+// floor(crd.z+0.5)) instead of the reference's y = z = floor(crd.x+0.5)
+// (:783), which in 3D lies elsewhere in the domain; on 1D grids both are the
+// same.
 double propagate_weno5(const Domain& D, const double crd[3], int i, const double* base, bool energy = false,
-                       bool row_fix = false) {
+                       bool centred = false) {
   const double fx = std::floor(crd[0] + 0.5), fy = std::floor(crd[1] + 0.5), fz = std::floor(crd[2] + 0.5);
-  const int64_t c0[3] = {(int64_t)(fx - 2), (int64_t)fy, (int64_t)fz};
-  const int64_t c1[3] = {(int64_t)(fx - 1), (int64_t)fy, (int64_t)fz};
-  const int64_t c2[3] = {(int64_t)(fx), (int64_t)fy, (int64_t)fz};
+  const double oy = centred ? fy - 1 : fy, oz = centred ? fz - 1 : fz;
+  const int64_t c0[3] = {(int64_t)(fx - 2), (int64_t)oy, (int64_t)oz};
+  const int64_t c1[3] = {(int64_t)(fx - 1), (int64_t)oy, (int64_t)oz};
+  const int64_t c2[3] = {(int64_t)(fx), (int64_t)oy, (int64_t)oz};
   const double S0 = lagr_eval(D, 3, crd, c0, i, base, energy);
   const double S1 = lagr_eval(D, 3, crd, c1, i, base, energy);
   const double S2 = lagr_eval(D, 3, crd, c2, i, base, energy);
@@ -447,7 +451,7 @@ double propagate_weno5(const Domain& D, const double crd[3], int i, const double
   const double d2 = (cdist * cdist + 3 * cdist + 2) / 12.;
   const double d1 = 1. - d0 - d2;
   // :783 -- the smoothness row uses y = z = floor(crd.x+0.5) (wrapped)
-  const int64_t lx = (int64_t)(fx - 2), ly = (int64_t)(row_fix ? fy : fx), lz = (int64_t)(row_fix ? fz : fx);
+  const int64_t lx = (int64_t)(fx - 2), ly = (int64_t)(centred ? fy : fx), lz = (int64_t)(centred ? fz : fx);
   double u[6];
   Cell c;
   for (int k = 1; k <= 5; k++) {

@@ -28,8 +28,9 @@ enum { ORC_LAGR2 = 2, ORC_LAGR3 = 3, ORC_LAGR4 = 4, ORC_LAGR5 = 5,
        ORC_WENO5 = 8,    /* propagateWENO<3,5> (steps.cu:774) */
        ORC_GAP2 = 9,     /* linear between the nearest active nodes, propagate_nonequal_1D<2> (steps.cu:1122) */
        ORC_NONUNIFORM3 = 10, /* quadratic on node positions, propagateNR_1D (steps.cu:882) */
-       ORC_WENO5_ROW = 11 }; /* propagateWENO<3,5> with the smoothness row through the departure
-                                point's own y, z (the reference's :783 reads row y = z = x) */
+       ORC_WENO5_ROW = 11 }; /* propagateWENO<3,5> centred: y, z windows floor(c+0.5)-1 .. +1 (the
+                                reference's :776-778 start at floor(c+0.5)) and the smoothness row
+                                through the departure point (the reference's :783 reads row y = z = x) */
 /* INFLOW: a ghost node below the low end holding the equilibrium of
    orc_params.inflow (rho, u_x, u_y, u_z, T), zero gradient above the high end */
 enum { ORC_BC_PERIODIC = 0, ORC_BC_CLAMP = 1, ORC_BC_MIRROR = 2, ORC_BC_INFLOW = 3 };
