@@ -560,8 +560,8 @@ def run_batch1d(steps=1000, nproblems=4096, pg=None, rank=0, world=1):
     drives most of these problems non-finite (the float64 oracle diverges on
     the same strong jumps), so the line also gives the rate over the node
     updates of problems still finite and the steps to divergence, and the same
-    measurement on a well-posed companion set (density ratio <= 10,
-    temperature ratio <= 2, moderate velocities).  Under several ranks the
+    measurement on a well-posed companion set (density ratio <= 4,
+    temperature ratio <= 1.5, moderate velocities).  Under several ranks the
     problems are split by node count (strong scaling: the whole set is the
     job) and the time is the slowest rank's."""
     from lbmpond_b200 import replicas
@@ -577,8 +577,8 @@ def run_batch1d(steps=1000, nproblems=4096, pg=None, rank=0, world=1):
         lengths, rho, u, T = lengths[mine], rho[sel], u[sel], T[sel]
         label = (f"{nproblems} D1Q5 Riemann problems, lengths U[256,4096] (seed 0), WENO5, {steps} steps"
                  if which == "specified" else
-                 f"{nproblems} moderate D1Q5 Riemann problems (density ratio <= 10, temperature ratio <= 2, "
-                 f"|u| <= 0.09, lattice T ~ 0.09), lengths U[256,4096] (seed 0), WENO5, {steps} steps")
+                 f"{nproblems} moderate D1Q5 Riemann problems (density ratio <= 4, temperature ratio <= 1.5, "
+                 f"|u| <= 0.06, lattice T ~ 0.09), lengths U[256,4096] (seed 0), WENO5, {steps} steps")
         rec = _batch_set(lengths, rho, u, T, steps, 50, pg, world, label)
         if which == "specified":
             out = rec

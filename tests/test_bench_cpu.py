@@ -43,8 +43,8 @@ def test_moderate_batch_set_bounds():
     off = np.concatenate([[0], np.cumsum(lengths)])
     for p in range(64):
         r, t, uu = rho[off[p]:off[p + 1]], T[off[p]:off[p + 1]], u[off[p]:off[p + 1]]
-        assert r.max() / r.min() <= 10 + 1e-9 and t.max() / t.min() <= 2 + 1e-9
-        assert np.abs(uu).max() <= 0.09 + 1e-12 and 0.09 / 2 ** 0.5 * 0.999 <= t.min()
+        assert r.max() / r.min() <= 4 + 1e-9 and t.max() / t.min() <= 1.5 + 1e-9
+        assert np.abs(uu).max() <= 0.06 + 1e-12 and 0.09 / 1.5 ** 0.5 * 0.999 <= t.min()
     # the specified set reaches ratios of up to 100 in rho and p
     lengths, rho, u, T = riemann_problems(64, seed=3)
     assert rho.max() / rho.min() > 10
