@@ -769,8 +769,9 @@ def run_configs_full(which, d3q125_size=192, l1_size_d3q125=48):
          against float64
       3  the batched D1Q5 problems (the benchmark line's batch1d)
       4  D3Q27 sphere 256^3, cubic, tau 0.52, 1500 steps: float32 plain and
-         learned (pairs from steps 121-150, the network attached from step 151)
-         against float64
+         learned (pairs from steps 121-150, the network attached from step 151);
+         each against the float64 path over ten steps from its final state (a
+         float64 run of the whole 1500 steps at 256^3 takes over half an hour)
       5  D3Q125 shock + vortex at d3q125_size^3, centred WENO5, inflow/outflow
          in x, 1000 steps, float32; L1 against float64 over ten steps from
          the final state (the float64 path at the reference's tolerance);
@@ -840,23 +841,34 @@ def run_configs_full(which, d3q125_size=192, l1_size_d3q125=48):
         out["batch1d"] = run_batch1d(1000, 4096)
         note("batch done")
     if "4" in which:
-        n, nsteps, spin = 256, 1500, 150
+        n, nsteps, spin, l1_steps = 256, 1500, 150, 10
         mk = lambda prec="fp32": pond.Solver(lattice="D3Q27", shape=(n,) * 3, interp=pond.LAGR4,  # noqa: E731
                                             precision=prec, tau=TAU, tol_abs=TOL_ABS if prec == "fp32" else None,
                                             tol_rel=TOL_REL if prec == "fp32" else None)
-        res = {}
-        with mk("fp64") as s:
-            s.init("sphere", *sphere_params())
-            d0 = s.diagnostics()
-            ms = _chunked(s, nsteps)
-            res["fp64"] = (s.fields(), _drift(d0, s.diagnostics(), nsteps), ms / nsteps, s.diagnostics())
-        note("sphere fp64 done")
+        rec = {"workload": f"D3Q27 {n}^3 spherical Riemann problem, tau {TAU}, cubic Lagrange, {nsteps} steps; "
+                           f"L1 against the float64 path over {l1_steps} steps from each run's final state"}
+
+        def l1_window(s):
+            """float32 against float64 over l1_steps steps from s's state (s advances)."""
+            with mk("fp64") as r:
+                r.copy_state_from(s)
+                d0 = r.diagnostics()
+                r.step(l1_steps)
+                fr = r.fields()
+                dr = _drift(d0, r.diagnostics(), l1_steps)
+                ms64 = r.last_step_ms() / l1_steps
+            s.step(l1_steps)
+            return {"window": f"steps {nsteps + 1}..{nsteps + l1_steps}", **_l1_fields(s.fields(), fr),
+                    "fp64_drift_in_window": dr, "fp64_ms_per_step": ms64}
+
         with mk() as s:
             s.init("sphere", *sphere_params())
             d0 = s.diagnostics()
             ms = _chunked(s, nsteps)
             d = s.diagnostics()
-            res["plain"] = (s.fields(), _drift(d0, d, nsteps), ms / nsteps, d)
+            rec["plain"] = {"ms_per_step": ms / nsteps, "MLUPS": n ** 3 / (ms / nsteps) / 1e3,
+                            "drift": _drift(d0, d, nsteps), "niter_mean_last_step": d["niter_mean"],
+                            "nonconverged_last_step": d["nonconverged"], "l1_vs_fp64": l1_window(s)}
         note("sphere plain done")
         cap = 4_000_000
         X = torch.empty((cap, 39), dtype=torch.float32, device="cuda")
@@ -879,21 +891,14 @@ def run_configs_full(which, d3q125_size=192, l1_size_d3q125=48):
             attach(s, net, gate=gate)
             ms_l = _chunked(s, nsteps - spin)
             d = s.diagnostics()
-            res["learned"] = (s.fields(), _drift(d0, d, nsteps), (ms + ms_l) / nsteps, d, ms_l / (nsteps - spin))
             attach(s, None)
             net.close()
+            rec["learned"] = {"ms_per_step": (ms + ms_l) / nsteps, "MLUPS": n ** 3 / ((ms + ms_l) / nsteps) / 1e3,
+                              "ms_per_step_after_attach": ms_l / (nsteps - spin),
+                              "MLUPS_after_attach": n ** 3 / (ms_l / (nsteps - spin)) / 1e3,
+                              "drift": _drift(d0, d, nsteps), "niter_mean_last_step": d["niter_mean"],
+                              "nonconverged_last_step": d["nonconverged"], "l1_vs_fp64": l1_window(s)}
         note("sphere learned done")
-        fr = res["fp64"][0]
-        rec = {"workload": f"D3Q27 {n}^3 spherical Riemann problem, tau {TAU}, cubic Lagrange, {nsteps} steps",
-               "fp64": {"ms_per_step": res["fp64"][2], "drift": res["fp64"][1],
-                        "niter_mean_last_step": res["fp64"][3]["niter_mean"]}}
-        for key in ("plain", "learned"):
-            r = res[key]
-            rec[key] = {"ms_per_step": r[2], "MLUPS": n ** 3 / r[2] / 1e3, "drift": r[1],
-                        "niter_mean_last_step": r[3]["niter_mean"], "nonconverged_last_step": r[3]["nonconverged"],
-                        "l1_vs_fp64": _l1_fields(r[0], fr)}
-        rec["learned"]["ms_per_step_after_attach"] = res["learned"][4]
-        rec["learned"]["MLUPS_after_attach"] = n ** 3 / res["learned"][4] / 1e3
         out["sphere_d3q27_256"] = rec
     if "5" in which:
         m, nsteps, l1_steps = d3q125_size, 1000, 10
