@@ -5,8 +5,12 @@
 // propagate<N>, N = 2, 3, 4), organised for the SM:
 //
 //  * a CTA owns a 32 x 4 x 2 tile of nodes and stages the tile plus a halo of
-//    2 nodes per side (36 x 8 x 6 nodes, 31 float planes: 27 populations,
-//    u_x, u_y, u_z and c = sqrts(T/TLat), 214 KB) once per step.  Boundary
+//    2 nodes per side (36 x 8 x 6 nodes) once per step, node-major: a staged
+//    node's 27 populations are contiguous and 16-byte aligned (a 28-float
+//    stride, 189 KB), so a lane fetches a stencil node with seven 16-byte
+//    loads, and the 28-word stride puts the eight lanes of every 16-byte load
+//    phase on distinct banks.  Each staging thread copies whole nodes and
+//    transfers them itself (no gauge planes in shared memory).  Boundary
 //    resolution (periodic wrap, clamp, mirror with population reversal), the
 //    reference's dropping of non-finite terms and the square root of T are
 //    applied while staging;
@@ -23,8 +27,10 @@
 //    per stencil column, x per stencil row: 81 FMA each) instead of
 //    transforming every stencil node into the target gauge (243 FMA);
 //  * the fixed-point iteration is warp-synchronous: a warp iterates while any
-//    of its lanes is unconverged, and walks the stencil offsets common to its
-//    lanes, so a warp's shared-memory loads hit 32 consecutive addresses;
+//    of its lanes is unconverged and walks the union of its lanes' stencil
+//    offsets, contracting every target class at every offset (a class a lane
+//    does not weight there has weight 0): straight-line code the scheduler
+//    interleaves;
 //  * a lane whose departure points leave the +-2 halo (|u| + sqrt(T/TLat) >= 1
 //    along an axis) runs that iteration from global memory instead.
 #pragma once
@@ -36,10 +42,13 @@ namespace d27 {
 constexpr int TX = 32, TY = 4, TZ = 2, H = 2;
 constexpr int SX = TX + 2 * H, SY = TY + 2 * H, SZ = TZ + 2 * H;
 constexpr int SN = SX * SY * SZ;  // 1728 staged nodes
-constexpr int NPL = 31;           // planes: 27 f, u_x, u_y, u_z, c
-// + a global node index (int32) and a flag byte per staged node
-constexpr size_t SMEM_BYTES = size_t(NPL) * SN * sizeof(float) + size_t(SN) * sizeof(int) + SN;
+constexpr int NS = 28;            // floats per staged node: its 27 R-gauge populations and a pad
 constexpr int THREADS = TX * TY * TZ;
+// staged nodes node-major (a node's populations contiguous, 16-byte aligned:
+// seven 16-byte loads per stencil node; the 28-word stride keeps the eight
+// lanes of each 16-byte load phase on distinct banks), then the iterate's
+// populations of every lane
+constexpr size_t SMEM_BYTES = size_t(NS) * SN * sizeof(float) + size_t(27) * THREADS * sizeof(float);
 
 // reference population index of tensor class t = 9 cx + 3 cy + cz, for
 // lookups with run-time indices (consts.h:20-30 order)
@@ -216,89 +225,98 @@ template <int N, bool kPartials = false>
 __global__ void __launch_bounds__(THREADS, 1) pull_d3q27_tile_kernel(StepArgs<float> a) {
   using L = Lattice<POND_D3Q27>;
   extern __shared__ __align__(16) float sm[];
-  int* gidx = reinterpret_cast<int*>(sm + NPL * SN);
-  unsigned char* flags = reinterpret_cast<unsigned char*>(gidx + SN);
   const int tid = threadIdx.x + TX * (threadIdx.y + TY * threadIdx.z);
   const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z0 = blockIdx.z * TZ;
 
-  // ---- stage the tile: every value is fetched with an asynchronous copy
-  // (cp.async, no register round trip), so a thread has all of its ~210
-  // copies in flight at once; boundary resolution happens in the addresses.
-  // 1) per staged node: global index, mirror flags, the four gauge planes
+  // ---- reference gauge of the CTA: the gauge of the tile's centre node
+  //      ((0, 1) if it is not finite or its c is 0)
+  float uref[3], icref;
+  {
+    bool rv[3];
+    const int gx = resolve_axis(x0 + TX / 2, a.nx, a.bc[0], rv[0]);
+    const int gy = resolve_axis(y0 + TY / 2, a.ny, a.bc[1], rv[1]);
+    const int gz = resolve_axis(z0 + TZ / 2, a.nz, a.bc[2], rv[2]);
+    const long long g = gx + (long long)a.nx * (gy + (long long)a.ny * gz);
+    const float T = a.g_in[3 * a.N + g];
+    const float cc = copysignf(sqrtf(fabsf(T) * (float)(1.0 / L::TLat)), T);
+    bool ok = fabsf(cc) <= 3.0e38f;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const float v = a.g_in[(long long)k * a.N + g];
+      uref[k] = rv[k] ? -v : v;
+      ok = ok && fabsf(v) <= 3.0e38f;
+    }
+#pragma unroll
+    for (int k = 0; k < 3; k++) uref[k] = ok ? uref[k] : 0.f;
+    icref = (ok && fabsf(cc) > 1.0e-20f) ? 1.f / cc : 1.f;
+  }
+  const float cref = 1.f / icref;
+
+  // ---- stage: each thread copies whole staged nodes (27 populations in
+  // tensor-class order, the mirror reversing classes) with asynchronous
+  // copies, waits for its own copies and transfers its nodes into the
+  // reference gauge; boundary resolution happens in the addresses, the gauge
+  // comes straight from global memory (mirrored velocity components flip; a
+  // node with a non-finite gauge contributes nothing, non-finite populations
+  // count as 0)
   for (int i = tid; i < SN; i += THREADS) {
     const int hx = i % SX, hy = (i / SX) % SY, hz = i / (SX * SY);
     bool rv[3];
     const int gx = resolve_axis(x0 - H + hx, a.nx, a.bc[0], rv[0]);
     const int gy = resolve_axis(y0 - H + hy, a.ny, a.bc[1], rv[1]);
     const int gz = resolve_axis(z0 - H + hz, a.nz, a.bc[2], rv[2]);
-    const int g = gx + a.nx * (gy + a.ny * gz);
-    gidx[i] = g;
-    flags[i] = (unsigned char)((rv[0] ? 1 : 0) | (rv[1] ? 2 : 0) | (rv[2] ? 4 : 0));
-#pragma unroll
-    for (int k = 0; k < 4; k++) cp_async4(&sm[(27 + k) * SN + i], a.g_in + (long long)k * a.N + g);
-  }
-  __syncthreads();
-  // 2) populations in tensor-class order (the mirror reverses classes)
-  for (int idx = tid; idx < 27 * SN; idx += THREADS) {
-    const int p = idx / SN, i = idx - p * SN;
-    const unsigned fl = flags[i];
-    int cx = p / 9, cy = (p / 3) % 3, cz = p % 3;
-    if (fl & 1) cx = rev3(cx);
-    if (fl & 2) cy = rev3(cy);
-    if (fl & 4) cz = rev3(cz);
-    cp_async4(&sm[idx], a.f_in + (long long)c_ref27[cx * 9 + cy * 3 + cz] * a.N + gidx[i]);
-  }
-  cp_async_wait_all();
-  __syncthreads();
-  // 3) gauge post-pass: mirrored velocity components flip sign, c = sqrts(T/TLat);
-  //    a node with a non-finite gauge contributes nothing (all its transfer
-  //    terms are non-finite in the reference and dropped)
-  for (int i = tid; i < SN; i += THREADS) {
-    const unsigned fl = flags[i];
-    float u[3];
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-      const float v = sm[(27 + k) * SN + i];
-      u[k] = (fl >> k) & 1 ? -v : v;
-    }
-    const float T = sm[30 * SN + i];
-    const float c = copysignf(sqrtf(fabsf(T) * (float)(1.0 / L::TLat)), T);
-    const bool ok = fabsf(u[0]) <= 3.0e38f && fabsf(u[1]) <= 3.0e38f && fabsf(u[2]) <= 3.0e38f && fabsf(c) <= 3.0e38f;
-    sm[27 * SN + i] = ok ? u[0] : 0.f;
-    sm[28 * SN + i] = ok ? u[1] : 0.f;
-    sm[29 * SN + i] = ok ? u[2] : 0.f;
-    sm[30 * SN + i] = ok ? c : 1.f;
-    flags[i] = (unsigned char)(fl | (ok ? 0 : 8));
-  }
-  __syncthreads();
-  // 4) reference gauge of the CTA: the gauge of the tile's centre node
-  //    (c = 1 if that node's c is 0)
-  float uref[3], icref;
-  {
-    constexpr int ci = (H + TZ / 2) * SX * SY + (H + TY / 2) * SX + (H + TX / 2);
-#pragma unroll
-    for (int k = 0; k < 3; k++) uref[k] = sm[(27 + k) * SN + ci];
-    const float cc = sm[30 * SN + ci];
-    icref = fabsf(cc) > 1.0e-20f ? 1.f / cc : 1.f;
-  }
-  const float cref = 1.f / icref;
-  // 5) populations -> transferred into the reference gauge, in place
-  //    (non-finite populations and every population of an invalid node count as 0)
-  for (int i = tid; i < SN; i += THREADS) {
-    const bool bad = flags[i] & 8;
-    float v[27];
+    const long long g = gx + (long long)a.nx * (gy + (long long)a.ny * gz);
 #pragma unroll
     for (int t = 0; t < 27; t++) {
-      const float x = sm[t * SN + i];
-      v[t] = (!bad && fabsf(x) <= 3.402823466e38f) ? x : 0.f;
+      int cx = t / 9, cy = (t / 3) % 3, cz = t % 3;
+      if (rv[0]) cx = rev3(cx);
+      if (rv[1]) cy = rev3(cy);
+      if (rv[2]) cz = rev3(cz);
+      cp_async4(&sm[i * NS + t], a.f_in + (long long)c_ref27[cx * 9 + cy * 3 + cz] * a.N + g);
     }
-    const float r = sm[30 * SN + i] * icref;
-    const float sq[3] = {(sm[27 * SN + i] - uref[0]) * icref, (sm[28 * SN + i] - uref[1]) * icref,
-                         (sm[29 * SN + i] - uref[2]) * icref};
+  }
+  cp_async_wait_all();
+  for (int i = tid; i < SN; i += THREADS) {
+    const int hx = i % SX, hy = (i / SX) % SY, hz = i / (SX * SY);
+    bool rv[3];
+    const int gx = resolve_axis(x0 - H + hx, a.nx, a.bc[0], rv[0]);
+    const int gy = resolve_axis(y0 - H + hy, a.ny, a.bc[1], rv[1]);
+    const int gz = resolve_axis(z0 - H + hz, a.nz, a.bc[2], rv[2]);
+    const long long g = gx + (long long)a.nx * (gy + (long long)a.ny * gz);
+    float u[3];
+    bool ok = true;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const float v = __ldg(&a.g_in[(long long)k * a.N + g]);
+      u[k] = rv[k] ? -v : v;
+      ok = ok && fabsf(v) <= 3.0e38f;
+    }
+    const float T = __ldg(&a.g_in[3 * a.N + g]);
+    const float c = copysignf(sqrtf(fabsf(T) * (float)(1.0 / L::TLat)), T);
+    ok = ok && fabsf(c) <= 3.0e38f;
+    float v[27];
+    {
+      const float4* s4 = reinterpret_cast<const float4*>(sm + i * NS);
+#pragma unroll
+      for (int q = 0; q < 7; q++) {
+        const float4 w = s4[q];
+        const float e[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+          if (4 * q + j < 27) v[4 * q + j] = (ok && fabsf(e[j]) <= 3.402823466e38f) ? e[j] : 0.f;
+      }
+    }
+    const float r = ok ? c * icref : 0.f;
+    const float sq[3] = {ok ? (u[0] - uref[0]) * icref : 0.f, ok ? (u[1] - uref[1]) * icref : 0.f,
+                         ok ? (u[2] - uref[2]) * icref : 0.f};
     const float rq[3] = {r, r, r};
     node_to_ref(v, sq, rq);
+    {
+      float4* s4 = reinterpret_cast<float4*>(sm + i * NS);
 #pragma unroll
-    for (int t = 0; t < 27; t++) sm[t * SN + i] = v[t];
+      for (int q = 0; q < 7; q++)
+        s4[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], 4 * q + 3 < 27 ? v[4 * q + 3] : 0.f);
+    }
   }
   __syncthreads();
 
@@ -307,11 +325,9 @@ __global__ void __launch_bounds__(THREADS, 1) pull_d3q27_tile_kernel(StepArgs<fl
   const bool active = x < a.nx && y < a.ny && z < a.nz;
   NodeSums ns = {0, 0, 0, 0, 0, 0, 0ull, 0ull, 0ull, 0};
   const long long idx = active ? x + (long long)a.nx * (y + (long long)a.ny * z) : 0;
-  // the node's current populations live in shared memory between iterations
-  // (the gauge planes are free once the staged nodes are transferred: 4 SN floats =
-  // 27 THREADS floats), which keeps them out of the loop's registers
-  static_assert(4 * SN == 27 * THREADS, "population store must fit the gauge planes");
-  float* f0s = sm + 27 * SN + tid;
+  // the node's current populations live in shared memory between iterations,
+  // which keeps them out of the loop's registers
+  float* f0s = sm + NS * SN + tid;
   double rho0 = 1, U[3] = {0, 0, 0}, T = L::TLat;
   {
     float f0[27];
@@ -368,41 +384,26 @@ __global__ void __launch_bounds__(THREADS, 1) pull_d3q27_tile_kernel(StepArgs<fl
         wl[ax] = __reduce_min_sync(0xffffffffu, done ? H : lo[ax]);
         wh[ax] = __reduce_max_sync(0xffffffffu, done ? -H : hi[ax]);
       }
-      // per axis, offset and target class: does any unconverged lane of the
-      // warp weight it (bit 3 (o + H) + class); classes nobody weights are skipped
-      unsigned need[3] = {0u, 0u, 0u};
-#pragma unroll
-      for (int ax = 0; ax < 3; ax++)
-#pragma unroll
-        for (int o = -H; o <= H; o++)
-#pragma unroll
-          for (int c = 0; c < 3; c++)
-            if (__any_sync(0xffffffffu, !done && wpick<N>(wt[ax][c], ro[ax][c], o) != 0.f))
-              need[ax] |= 1u << (3 * (o + H) + c);
+      // every target class at every offset (a class a lane does not weight
+      // there gets weight 0): branch-free contractions the scheduler can
+      // interleave, which measured faster than skipping the classes no lane
+      // of the warp weights (54.8 against 58.8 ms per 256^3 step)
+      const bool all3[3] = {true, true, true};
       if (!done) {  // floating-point operations of the contractions below
         const unsigned long long ex = wh[0] - wl[0] + 1, ey = wh[1] - wl[1] + 1, ez = wh[2] - wl[2] + 1;
-        work += ex * ey * (54ull * __popc(need[2]) + 9 * ez) + ex * (54ull * __popc(need[1]) + 9 * ey) +
-                54ull * __popc(need[0]) + 9 * ex;
+        work += ex * ey * ez * (54ull * 3 + 9) + ex * ey * (54ull * 3 + 9) + ex * (54ull * 3 + 9);
       }
       for (int ox = wl[0]; ox <= wh[0]; ox++) {
         float wx[3];
-        bool nx[3];
 #pragma unroll
-        for (int c = 0; c < 3; c++) {
-          wx[c] = wpick<N>(wt[0][c], ro[0][c], ox);
-          nx[c] = (need[0] >> (3 * (ox + H) + c)) & 1u;
-        }
+        for (int c = 0; c < 3; c++) wx[c] = wpick<N>(wt[0][c], ro[0][c], ox);
         float Yr[27];
 #pragma unroll
         for (int t = 0; t < 27; t++) Yr[t] = 0.f;
         for (int oy = wl[1]; oy <= wh[1]; oy++) {
           float wy[3];
-          bool ny[3];
 #pragma unroll
-          for (int c = 0; c < 3; c++) {
-            wy[c] = wpick<N>(wt[1][c], ro[1][c], oy);
-            ny[c] = (need[1] >> (3 * (oy + H) + c)) & 1u;
-          }
+          for (int c = 0; c < 3; c++) wy[c] = wpick<N>(wt[1][c], ro[1][c], oy);
           float Zc[27];
 #pragma unroll
           for (int t = 0; t < 27; t++) Zc[t] = 0.f;
@@ -410,22 +411,24 @@ __global__ void __launch_bounds__(THREADS, 1) pull_d3q27_tile_kernel(StepArgs<fl
           for (int oz = -H; oz <= H; oz++) {
             if (oz < wl[2] || oz > wh[2]) continue;
             float wz[3];
-            bool nz[3];
 #pragma unroll
-            for (int c = 0; c < 3; c++) {
-              wz[c] = wpick<N>(wt[2][c], ro[2][c], oz);
-              nz[c] = (need[2] >> (3 * (oz + H) + c)) & 1u;
+            for (int c = 0; c < 3; c++) wz[c] = wpick<N>(wt[2][c], ro[2][c], oz);
+            const float4* s4 = reinterpret_cast<const float4*>(sm + (sbase + oz * SX * SY + oy * SX + ox) * NS);
+            float vv[28];
+#pragma unroll
+            for (int q = 0; q < 7; q++) {
+              const float4 w = s4[q];
+              vv[4 * q] = w.x; vv[4 * q + 1] = w.y; vv[4 * q + 2] = w.z; vv[4 * q + 3] = w.w;
             }
-            const float* sv = sm + (sbase + oz * SX * SY + oy * SX + ox);
-            contract_z(Gz, wz, nz, [&](int t) { return sv[t * SN]; }, Zc);
+            contract_z(Gz, wz, all3, [&](int t) { return vv[t]; }, Zc);
           }
           float Gy[3][3];
           basis_rows(bq[1], ainv, Gy);
-          contract_y(Gy, wy, ny, Zc, Yr);
+          contract_y(Gy, wy, all3, Zc, Yr);
         }
         float Gx[3][3];
         basis_rows(bq[0], ainv, Gx);
-        contract_x(Gx, wx, nx, Yr, acc);
+        contract_x(Gx, wx, all3, Yr, acc);
       }
     } else if (!done) {
       // departure points beyond the staged halo: this lane reads global memory
