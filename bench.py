@@ -664,7 +664,7 @@ def run_configs(steps=5, warmup=2, d3q125_size=48):
                                 "niter_max": d["niter_max"], "steps_timed": f"{warmup + 1}..{warmup + steps}"}
     note("tgv done")
     # the same vortex as a gamma = 1.4 gas: energy populations with 2 extra degrees of freedom
-    # (one thread per node: the staged tile kernel has no room for them)
+    # (the energy tile kernel: the f and h of each node on two paired warps)
     T14 = (1.0 / 3.0) / 4
     U14 = 0.5 * np.sqrt(1.4 * T14)
     with pond.Solver(lattice="D3Q27", shape=(128,) * 3, precision="fp32", interp=pond.LAGR3, tau=0.51,
@@ -865,17 +865,19 @@ def run_configs_full(which, d3q125_size=192, l1_size_d3q125=48):
                     "fp64_drift_in_window": dr, "fp64_ms_per_step": ms64}
 
         def progress(s, label, k, ms):
-            d = s.diagnostics()
+            d, fl = s.diagnostics(), s.fields()
+            umax = np.sqrt(fl["ux"] ** 2 + fl["uy"] ** 2 + fl["uz"] ** 2).max()
             note(f"{label} step {k}: {ms:.0f} ms so far, niter mean {d['niter_mean']:.3f} max {d['niter_max']} "
-                 f"nonconverged {d['nonconverged']}")
+                 f"nonconverged {d['nonconverged']}, T {fl['T'].min():.4g}..{fl['T'].max():.4g}, max |u| {umax:.4g}, "
+                 f"rho {fl['rho'].min():.4g}..{fl['rho'].max():.4g}")
 
         with mk() as s:
             s.init("sphere", *sphere_params())
             d0 = s.diagnostics()
             ms, done = 0.0, 0
-            for k0 in range(0, nsteps, 100):
-                ms += _chunked(s, min(100, nsteps - k0))
-                done = min(k0 + 100, nsteps)
+            for k0 in range(0, nsteps, 25):
+                ms += _chunked(s, min(25, nsteps - k0))
+                done = min(k0 + 25, nsteps)
                 progress(s, "plain", done, ms)
                 if not np.isfinite(s.diagnostics()["mass"]):
                     break
@@ -1066,8 +1068,9 @@ def run_reference(args, rank, world):
     return {"impl": "reference", "metric": METRIC, "value": v, "unit": "MLUPS", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"D3Q27 spherical Riemann problem (sample {m}^3), tau {TAU}, cubic Lagrange",
-                       "path": "reference step on the host"},
+            "config": {"workload": f"D3Q27 {args.size}^3 spherical Riemann problem, tau {TAU}, cubic Lagrange, "
+                                   f"tolerance {TOL_ABS:g}+{TOL_REL:g}|v|",
+                       "path": "reference step on the host", "sample": sample},
             "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 

@@ -10,6 +10,7 @@
 #include "pond_step_1d_energy.cuh"
 #include "pond_step_1d_mesh.cuh"
 #include "pond_step_d3q27_energy.cuh"
+#include "pond_step_d3q27_energy_tile.cuh"
 #include "pond_step_d3q125_tile.cuh"
 #include "pond_step_d3q27.cuh"
 #include "pond_step_point.cuh"
@@ -235,6 +236,20 @@ template <typename R> static int launch_typed(pond_ctx* c, const void* const* in
       return set_error(POND_ERR_UNSUPPORTED, "energy populations on D3Q125 run in float32");
     }
     if (c->p.lattice == POND_D3Q27) {
+      if constexpr (std::is_same<R, float>::value) {
+        if (c->p.interp == POND_LAGR2 || c->p.interp == POND_LAGR3 || c->p.interp == POND_LAGR4) {
+          const dim3 grd((a.nx + d27e::TX - 1) / d27e::TX, (a.ny + d27e::TY - 1) / d27e::TY,
+                         (a.nz + d27e::TZ - 1) / d27e::TZ);
+          auto kern = c->p.interp == POND_LAGR2   ? d27e::pull_d3q27_energy_tile_kernel<2>
+                      : c->p.interp == POND_LAGR3 ? d27e::pull_d3q27_energy_tile_kernel<3>
+                                                  : d27e::pull_d3q27_energy_tile_kernel<4>;
+          e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d27e::SMEM_BYTES);
+          if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+          kern<<<grd, d27e::THREADS, d27e::SMEM_BYTES, s>>>(a);
+          e = cudaGetLastError();
+          return e == cudaSuccess ? POND_OK : cuda_fail(e, "step kernel launch");
+        }
+      }
       const dim3 blk(32, 4, 1), grd((a.nx + 31) / 32, (a.ny + 3) / 4, a.nz);
       switch (c->p.interp) {
         case POND_LAGR2: pull_d3q27_energy_kernel<2, R><<<grd, blk, 0, s>>>(a); break;

@@ -433,10 +433,11 @@ __global__ void __launch_bounds__(THREADS, 1) pull_d3q27_tile_kernel(StepArgs<fl
     } else if (!done) {
       // departure points beyond the staged halo: this lane reads global memory
       // and transfers each stencil node into the reference gauge itself
-      const unsigned long long ex = hi[0] - lo[0] + 1, ey = hi[1] - lo[1] + 1, ez = hi[2] - lo[2] + 1;
+      const unsigned long long ex = window_positions<N, 3>(ro[0]), ey = window_positions<N, 3>(ro[1]),
+                               ez = window_positions<N, 3>(ro[2]);
       work += ex * ey * ez * 171 + ex * ey * 171 + ex * 171;
       const bool all3[3] = {true, true, true};
-      for (int ox = lo[0]; ox <= hi[0]; ox++) {
+      for (int ox = lo[0]; ox <= hi[0]; ox = window_next<N, 3>(ro[0], ox)) {
         bool rv[3] = {false, false, false};
         const int gx = resolve_axis(x + ox, a.nx, a.bc[0], rv[0]);
         float wx[3];
@@ -445,7 +446,7 @@ __global__ void __launch_bounds__(THREADS, 1) pull_d3q27_tile_kernel(StepArgs<fl
         float Yr[27];
 #pragma unroll
         for (int t = 0; t < 27; t++) Yr[t] = 0.f;
-        for (int oy = lo[1]; oy <= hi[1]; oy++) {
+        for (int oy = lo[1]; oy <= hi[1]; oy = window_next<N, 3>(ro[1], oy)) {
           const int gy = resolve_axis(y + oy, a.ny, a.bc[1], rv[1]);
           float wy[3];
 #pragma unroll
@@ -453,7 +454,7 @@ __global__ void __launch_bounds__(THREADS, 1) pull_d3q27_tile_kernel(StepArgs<fl
           float Zc[27];
 #pragma unroll
           for (int t = 0; t < 27; t++) Zc[t] = 0.f;
-          for (int oz = lo[2]; oz <= hi[2]; oz++) {
+          for (int oz = lo[2]; oz <= hi[2]; oz = window_next<N, 3>(ro[2], oz)) {
             const int gz = resolve_axis(z + oz, a.nz, a.bc[2], rv[2]);
             float wz[3];
 #pragma unroll

@@ -108,19 +108,20 @@ __global__ void __launch_bounds__(128) pull_d3q27_energy_kernel(StepArgs<R> a) {
         lo[ax] = min(org[ax][0], min(org[ax][1], org[ax][2]));
         hi[ax] = max(org[ax][0], max(org[ax][1], org[ax][2])) + N - 1;
       }
-      ns.work += (unsigned long long)(hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
-      for (int px = lo[0]; px <= hi[0]; px++) {
+      ns.work += (unsigned long long)window_positions<N, Q1>(org[0]) * window_positions<N, Q1>(org[1]) *
+                 window_positions<N, Q1>(org[2]);
+      for (int px = lo[0]; px <= hi[0]; px = window_next<N, Q1>(org[0], px)) {
         bool rv[3] = {false, false, false};
         const int rx = resolve_axis(px, dims[0], a.bc[0], rv[0]);
         R wx[Q1];
 #pragma unroll
         for (int c = 0; c < Q1; c++) wx[c] = pick<N, R>(wt[0][c], org[0][c], px);
-        for (int py = lo[1]; py <= hi[1]; py++) {
+        for (int py = lo[1]; py <= hi[1]; py = window_next<N, Q1>(org[1], py)) {
           const int ry = resolve_axis(py, dims[1], a.bc[1], rv[1]);
           R wy[Q1];
 #pragma unroll
           for (int c = 0; c < Q1; c++) wy[c] = pick<N, R>(wt[1][c], org[1][c], py);
-          for (int pz = lo[2]; pz <= hi[2]; pz++) {
+          for (int pz = lo[2]; pz <= hi[2]; pz = window_next<N, Q1>(org[2], pz)) {
             const int rz = resolve_axis(pz, dims[2], a.bc[2], rv[2]);
             R wz[Q1];
 #pragma unroll

@@ -43,10 +43,45 @@ template <int N, typename R> __device__ __forceinline__ void lagr_weights(double
 // Window origin of propagate<N> along one axis (steps.cu:996-997: even N use
 // floor(c)-N/2+1; odd N use floor(c+0.5)-(N-1)/2 in x and floor(c)-(N-1)/2
 // in y and z).
+// A coordinate beyond +-2^29 (a diverged gauge) is held there, so origins,
+// offsets and the positions built from them stay inside int; a NaN stays NaN.
 template <int N> __device__ __forceinline__ int window_origin(double c, int axis) {
+  if (fabs(c) > 536870912.0) c = copysign(536870912.0, c);
   if (N % 2 == 0) return (int)(floor(c) - N / 2 + 1);
   if (axis == 0) return (int)(floor(c + 0.5) - (N - 1) / 2);
   return (int)(floor(c) - (N - 1) / 2);
+}
+
+// The stencil positions of one axis are the union of the Q1 class windows
+// [org[c], org[c] + N), walked in increasing order from the lowest origin:
+// the position after p is p + 1 when a window holds it, else the next origin
+// above p (INT_MAX past the last window).  The walk visits at most Q1 N
+// positions however far a hot or fast node's gauge spreads the windows,
+// where a sweep over every position between the lowest and the highest
+// window would grow with the spread.
+template <int N, int Q1> __device__ __forceinline__ int window_next(const int org[Q1], int p) {
+  const int q = p + 1;
+  bool in = false;
+  int nxt = 0x7fffffff;
+#pragma unroll
+  for (int c = 0; c < Q1; c++) {
+    in = in || (q - org[c] >= 0 && q - org[c] < N);
+    nxt = org[c] > p ? min(nxt, org[c]) : nxt;
+  }
+  return in ? q : nxt;
+}
+// number of positions the walk visits
+template <int N, int Q1> __device__ __forceinline__ int window_positions(const int org[Q1]) {
+  int n = 0;
+#pragma unroll
+  for (int k = 0; k < Q1 * N; k++) {
+    const int c = k / N, p = org[c] + k % N;
+    bool seen = false;
+#pragma unroll
+    for (int c2 = 0; c2 < c; c2++) seen = seen || (p - org[c2] >= 0 && p - org[c2] < N);
+    n += seen ? 0 : 1;
+  }
+  return n;
 }
 
 // weight of window position j for a node at coordinate p (0 outside the window)
@@ -329,21 +364,22 @@ __global__ void __launch_bounds__(128) pull_point_kernel(StepArgs<R> a) {
           lo[ax] = hi[ax] = pos[ax];
         }
       }
-      ns.work += (unsigned long long)(hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
-      for (int px = lo[0]; px <= hi[0]; px++) {
+      ns.work += (unsigned long long)window_positions<N, Q1>(org[0]) *
+                 (D == 3 ? window_positions<N, Q1>(org[1]) * window_positions<N, Q1>(org[2]) : 1);
+      for (int px = lo[0]; px <= hi[0]; px = window_next<N, Q1>(org[0], px)) {
         bool rv[3] = {false, false, false};
         const int rx = resolve_axis((int)px, dims[0], a.bc[0], rv[0]);
         R wx[Q1];
 #pragma unroll
         for (int c = 0; c < Q1; c++) wx[c] = pick<N, R>(wt[0][c], org[0][c], px);
-        for (int py = lo[1]; py <= hi[1]; py++) {
+        for (int py = lo[1]; py <= hi[1]; py = D == 3 ? window_next<N, Q1>(org[1], py) : py + 1) {
           const int ry = (D == 3) ? resolve_axis((int)py, dims[1], a.bc[1], rv[1]) : (int)py;
           R wy[Q1];
           if (D == 3) {
 #pragma unroll
             for (int c = 0; c < Q1; c++) wy[c] = pick<N, R>(wt[1][c], org[1][c], py);
           }
-          for (int pz = lo[2]; pz <= hi[2]; pz++) {
+          for (int pz = lo[2]; pz <= hi[2]; pz = D == 3 ? window_next<N, Q1>(org[2], pz) : pz + 1) {
             const int rz = (D == 3) ? resolve_axis((int)pz, dims[2], a.bc[2], rv[2]) : (int)pz;
             const long long nidx = rx + (long long)a.nx * (ry + (long long)a.ny * rz);
             R fn[Q], s[3], r[3];

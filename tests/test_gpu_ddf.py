@@ -96,6 +96,53 @@ def test_d3q27_energy_step_matches_oracle(orc, pond, interp, shape, bc, precisio
     assert abs(d["enrg"] - total) <= 1e-6 * abs(total)
 
 
+@pytest.mark.parametrize("interp,bc", [(2, (0, 2, 1)), (3, (2, 0, 0)), (4, (0, 0, 0)), (4, (1, 2, 2))])
+def test_d3q27_energy_tile_spans_several_ctas(orc, pond, interp, bc):
+    """The float32 energy tile kernel (8 x 4 x 4 nodes per CTA, f and h on
+    paired warps) on a box of 3 x 3 x 3 ragged tiles."""
+    dof, tau, shape = 2, 0.7, (20, 9, 10)
+    rho, g = smooth_state(shape, 3, seed=20 + interp, modes=2, du=0.04, T0=0.2)
+    f = perturbed_populations(orc, 1, rho, g, seed=20 + interp, eps=0.01)
+    st = orc.with_energy(orc.State(f, rho, g), 1, dof)
+    st.h = st.h * (1 + 0.01 * np.random.default_rng(11).standard_normal(st.h.shape))
+    names = {0: "periodic", 1: "clamp", 2: "mirror"}
+    with pond.Solver(lattice="D3Q27", shape=shape, interp=interp, precision="fp32", tau=tau,
+                     bc=tuple(names[b] for b in bc), ddf_dof=dof) as s:
+        s.set_state(st.rho, st.g, f=st.f)
+        s.set_energy(st.h)
+        ref = st
+        for _ in range(3):
+            s.step(1)
+            ref, niter, nc = orc.step(ref, 1, shape, interp=interp, tau=tau, bc=bc, dof=dof,
+                                      tol_abs=s.params.tol_abs, tol_rel=s.params.tol_rel)
+        err = _errors(s, ref)
+        d = s.diagnostics()
+    assert all(v <= TOL["fp32"] for v in err.values()), err
+    assert d["nonconverged"] == 0 and d["niter_max"] >= 2
+
+
+@pytest.mark.parametrize("interp", [2, 3, 4])
+def test_d3q27_energy_departures_beyond_staged_halo(orc, pond, interp):
+    """A fast, hot flow sends departure points past the energy tile's +-2
+    halo; those lanes read f and h from global memory."""
+    dof, tau, shape = 2, 0.8, (40, 6, 4)
+    rho, g = smooth_state(shape, 3, seed=9, modes=1, du=0.05)
+    g[0] += 0.75
+    g[3] = 0.12 * (1 + 0.1 * np.sin(np.arange(rho.size)))
+    f = perturbed_populations(orc, 1, rho, g, seed=9, eps=0.01)
+    st = orc.with_energy(orc.State(f, rho, g), 1, dof)
+    with pond.Solver(lattice="D3Q27", shape=shape, interp=interp, precision="fp32", tau=tau, ddf_dof=dof) as s:
+        s.set_state(st.rho, st.g, f=st.f)
+        s.set_energy(st.h)
+        ref = st
+        for _ in range(2):
+            s.step(1)
+            ref, niter, nc = orc.step(ref, 1, shape, interp=interp, tau=tau, dof=dof,
+                                      tol_abs=s.params.tol_abs, tol_rel=s.params.tol_rel)
+        err = _errors(s, ref)
+    assert all(v <= TOL["fp32"] for v in err.values()), err
+
+
 @pytest.mark.parametrize("shape,bc", [((5, 4, 4), (0, 0, 0)), ((9, 6, 5), (1, 0, 2))])
 def test_d3q125_energy_step_matches_oracle(orc, pond, shape, bc):
     """The staged D3Q125 tile kernel with energy populations (float32)."""
