@@ -101,7 +101,7 @@ typedef struct {
   int device;      /* CUDA device ordinal */
   int learned;     /* 1: start each node's iteration from the predictor's gauge */
   int ddf;         /* 1: energy populations (double-distribution extension; D1Q5 on 1D grids,
-                      D3Q27 with Lagrange 2-5, D3Q125 in float32): a second
+                      D3Q27 with Lagrange 2-5, D3Q125 fixed-origin quadratic): a second
                       population set carries the total energy, gamma = (Dim+dof+2)/(Dim+dof);
                       completes the reference's DDF scaffolding (structs.cuh:37-39,336-341,391-394,
                       lbpack.cu:18-20, steps.cu:233-236) */

@@ -283,10 +283,9 @@ int pond_create(const pond_params* p, pond_ctx** out) {
   if (p->ddf) {
     const bool d1 = p->lattice == POND_D1Q5 && p->Ny == 1 && p->Nz == 1;
     const bool d27 = p->lattice == POND_D3Q27 && p->interp >= POND_LAGR2 && p->interp <= POND_LAGR5;
-    const bool d125 = p->lattice == POND_D3Q125 && p->precision == POND_FP32;
+    const bool d125 = p->lattice == POND_D3Q125;
     if (!d1 && !d27 && !d125)
-      return set_error(POND_ERR_UNSUPPORTED,
-                       "energy populations run on D1Q5 1D grids, D3Q27 (Lagrange 2-5) and D3Q125 (float32)");
+      return set_error(POND_ERR_UNSUPPORTED, "energy populations run on D1Q5 1D grids, D3Q27 (Lagrange 2-5) and D3Q125");
     if (p->ddf_dof < 0 || p->ddf_dof > 1000) return set_error(POND_ERR_ARG, "ddf_dof must be in 0..1000");
     if (p->learned) return set_error(POND_ERR_UNSUPPORTED, "the learned start does not carry energy populations");
   }

@@ -232,8 +232,17 @@ template <typename R> static int launch_typed(pond_ctx* c, const void* const* in
         d125t::pull_d3q125_tile_kernel<true><<<grd, d125t::THREADS, smem, s>>>(a);
         e = cudaGetLastError();
         return e == cudaSuccess ? POND_OK : cuda_fail(e, "step kernel launch");
+      } else {  // float64: 2^3 tiles, the two population sets of a 4^3 tile would not fit
+        constexpr int TT = 2;
+        const size_t smem = sizeof(d125t::SmemT<true, double, TT>);
+        e = cudaFuncSetAttribute(d125t::pull_d3q125_tile_kernel<true, double, TT>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+        const dim3 grd((a.nx + TT - 1) / TT, (a.ny + TT - 1) / TT, (a.nz + TT - 1) / TT);
+        d125t::pull_d3q125_tile_kernel<true, double, TT><<<grd, d125t::THREADS, smem, s>>>(a);
+        e = cudaGetLastError();
+        return e == cudaSuccess ? POND_OK : cuda_fail(e, "step kernel launch");
       }
-      return set_error(POND_ERR_UNSUPPORTED, "energy populations on D3Q125 run in float32");
     }
     if (c->p.lattice == POND_D3Q27) {
       if constexpr (std::is_same<R, float>::value) {

@@ -44,19 +44,23 @@ constexpr int PS = SN + 1;          // plane stride: 25 * 217 = 17 mod 32
 constexpr int WARPS = 8;
 constexpr int THREADS = 32 * WARPS;
 
-template <bool kE, typename Rs = float> struct SmemT {
-  Rs f[125 * PS];          // staged populations (non-finite values zeroed), then their transfer into R
-  Rs h[kE ? 125 * PS : 1]; // the same for the energy populations (double-distribution extension)
-  Rs u[3][SN];             // staged velocities (sign-flipped on mirrored axes)
-  Rs c[SN];                // sqrts(T / TLat)
-  unsigned char flags[SN]; // mirrored axes (bits 0-2)
-  Rs GY[WARPS][3][25];     // per warp and iteration: y weight x transfer entry, [n_y][5 i2 + k2]
+// TT: tile edge (4; 2 for the float64 tile with energy populations, whose
+// two population sets of a 4^3 tile would not fit)
+template <bool kE, typename Rs = float, int TT = T> struct SmemT {
+  static constexpr int SNT = (TT + 2) * (TT + 2) * (TT + 2), PST = SNT + 1;
+  Rs f[125 * PST];          // staged populations (non-finite values zeroed), then their transfer into R
+  Rs h[kE ? 125 * PST : 1]; // the same for the energy populations (double-distribution extension)
+  Rs u[3][SNT];             // staged velocities (sign-flipped on mirrored axes)
+  Rs c[SNT];                // sqrts(T / TLat)
+  unsigned char flags[SNT]; // mirrored axes (bits 0-2)
+  Rs GY[WARPS][3][25];      // per warp and iteration: y weight x transfer entry, [n_y][5 i2 + k2]
 };
 using Smem = SmemT<false>;
 
 static_assert(2 * (sizeof(SmemT<false>) + 1024) <= 233472, "two CTAs must fit in the 228 KB of an SM");
 static_assert(sizeof(SmemT<true>) + 1024 <= 233472, "the energy variant must fit one CTA per SM");
 static_assert(sizeof(SmemT<false, double>) <= 232448, "the float64 tile must fit one CTA");
+static_assert(sizeof(SmemT<true, double, 2>) <= 232448, "the float64 energy tile must fit one CTA");
 
 // one axis of a staged position: the index, with the inflow boundary's
 // ghost below the low end (*ghost) and zero gradient above the high end
@@ -69,10 +73,11 @@ __device__ __forceinline__ int staged_axis(int p, int n, int bc, bool& rev, bool
   return resolve_axis(p, n, bc, rev);
 }
 
-// global node of staged node i and its mirror flags; -1 for the inflow ghost
-template <typename Rs>
+// global node of staged node i (staged edge SS) and its mirror flags; -1 for
+// the inflow ghost
+template <int SS, typename Rs>
 __device__ __forceinline__ int staged_global(const StepArgs<Rs>& a, int x0, int y0, int z0, int i, bool rv[3]) {
-  const int hx = i % S, hy = (i / S) % S, hz = i / (S * S);
+  const int hx = i % SS, hy = (i / SS) % SS, hz = i / (SS * SS);
   bool ghost = false;
   const int gx = staged_axis(x0 - 1 + hx, a.nx, a.bc[0], rv[0], ghost);
   const int gy = staged_axis(y0 - 1 + hy, a.ny, a.bc[1], rv[1], ghost);
@@ -114,21 +119,23 @@ __device__ __forceinline__ void stencil_weights(int pos, double C, double U, int
 
 // kE: with the energy populations of the double-distribution extension
 // (staged, transferred and contracted like f; T from their sum; one CTA per SM).
-// R: storage and transfer type (float64: one CTA per SM, no energy variant).
-template <bool kE, typename R = float>
+// R: storage and transfer type (float64: one CTA per SM).
+// TT: tile edge (2 for the float64 energy variant: 8 nodes, one per warp).
+template <bool kE, typename R = float, int TT = T>
 __global__ void __launch_bounds__(THREADS, (kE || sizeof(R) == 8) ? 1 : 2) pull_d3q125_tile_kernel(StepArgs<R> a) {
-  static_assert(!(kE && sizeof(R) == 8), "the float64 tile has no room for energy populations");
+  static_assert(!(kE && sizeof(R) == 8 && TT > 2), "a float64 4^3 tile has no room for energy populations");
+  constexpr int S = TT + 2, SN = S * S * S, PS = SN + 1;  // staged edge, staged nodes, plane stride
   using L = Lattice<POND_D3Q125>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  SmemT<kE, R>& sm = *reinterpret_cast<SmemT<kE, R>*>(smem_raw);
+  SmemT<kE, R, TT>& sm = *reinterpret_cast<SmemT<kE, R, TT>*>(smem_raw);
   const R kFinMax = R(sizeof(R) == 8 ? 1.7976931348623157e308 : 3.402823466e38);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int x0 = blockIdx.x * T, y0 = blockIdx.y * T, z0 = blockIdx.z * T;
+  const int x0 = blockIdx.x * TT, y0 = blockIdx.y * TT, z0 = blockIdx.z * TT;
 
   // ---- stage the tile (steps.cu:164-193 per node, once per CTA here)
   for (int i = tid; i < SN; i += THREADS) {
     bool rv[3];
-    const int g = staged_global(a, x0, y0, z0, i, rv);
+    const int g = staged_global<S>(a, x0, y0, z0, i, rv);
     sm.flags[i] = (unsigned char)((rv[0] ? 1 : 0) | (rv[1] ? 2 : 0) | (rv[2] ? 4 : 0));
 #pragma unroll
     for (int k = 0; k < 3; k++) {
@@ -141,7 +148,7 @@ __global__ void __launch_bounds__(THREADS, (kE || sizeof(R) == 8) ? 1 : 2) pull_
   for (int idx = tid; idx < 125 * SN; idx += THREADS) {
     const int p = idx / SN, i = idx - p * SN;
     bool rv[3];
-    const int g = staged_global(a, x0, y0, z0, i, rv);
+    const int g = staged_global<S>(a, x0, y0, z0, i, rv);
     if (g < 0) {  // the inflow ghost: set_base of the inflow state (and its energy equilibrium)
       const double w = lattice_weight_t<POND_D3Q125>(p);
       sm.f[p * PS + i] = R(a.inflow[0] * w);
@@ -162,8 +169,12 @@ __global__ void __launch_bounds__(THREADS, (kE || sizeof(R) == 8) ? 1 : 2) pull_
                    : "memory");
     if constexpr (kE) {
       const unsigned dh = static_cast<unsigned>(__cvta_generic_to_shared(&sm.h[p * PS + i]));
-      asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dh), "l"(a.h_in + (long long)p * a.N + g)
-                   : "memory");
+      if constexpr (sizeof(R) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dh), "l"(a.h_in + (long long)p * a.N + g)
+                     : "memory");
+      else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dh), "l"(a.h_in + (long long)p * a.N + g)
+                     : "memory");
     }
   }
   asm volatile("cp.async.wait_all;\n" ::: "memory");
@@ -176,11 +187,11 @@ __global__ void __launch_bounds__(THREADS, (kE || sizeof(R) == 8) ? 1 : 2) pull_
   }
   __syncthreads();
 
-  // ---- reference gauge R: the staged node at tile position (2, 2, 2)
+  // ---- reference gauge R: the staged node at tile position (TT/2, TT/2, TT/2)
   //      ((0, 1) if that node's gauge is not finite or its c is 0)
   R uref[3], cref;
   {
-    constexpr int ci = ((2 + 1) * S + (2 + 1)) * S + (2 + 1);
+    constexpr int cp = TT / 2 + 1, ci = (cp * S + cp) * S + cp;
     const R cc = sm.c[ci];
     bool ok = fabs(cc) <= kFinMax && fabs(cc) > 1.0e-20f;
 #pragma unroll
@@ -267,8 +278,8 @@ __global__ void __launch_bounds__(THREADS, (kE || sizeof(R) == 8) ? 1 : 2) pull_
   const bool worker = lane < 25;
   const int j = worker ? lane / 5 : 4, k = lane % 5;
   NodeSums ns = {0, 0, 0, 0, 0, 0, 0ull, 0ull, 0ull, 0};
-  for (int t = warp; t < T * T * T; t += WARPS) {
-    const int lx = t % T, ly = (t / T) % T, lz = t / (T * T);
+  for (int t = warp; t < TT * TT * TT; t += WARPS) {
+    const int lx = t % TT, ly = (t / TT) % TT, lz = t / (TT * TT);
     const int x = x0 + lx, y = y0 + ly, z = z0 + lz;
     if (x >= a.nx || y >= a.ny || z >= a.nz) continue;  // warp-uniform
     const long long idx = x + (long long)a.nx * (y + (long long)a.ny * z);

@@ -1,7 +1,7 @@
 """GPU parity of the double-distribution extension (energy populations) with
 the float64 oracle, through the C ABI.
 
-A D1Q5, D3Q27 or (float32) D3Q125 context made with ``ddf_dof`` carries energy
+A D1Q5, D3Q27 or D3Q125 context made with ``ddf_dof`` carries energy
 populations h beside f;
 its temperature comes from them and gamma = (Dim + dof + 2) / (Dim + dof).
 The oracle restates the same extension (``orc.step(..., dof=...)``); both are
@@ -143,16 +143,18 @@ def test_d3q27_energy_departures_beyond_staged_halo(orc, pond, interp):
     assert all(v <= TOL["fp32"] for v in err.values()), err
 
 
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
 @pytest.mark.parametrize("shape,bc", [((5, 4, 4), (0, 0, 0)), ((9, 6, 5), (1, 0, 2))])
-def test_d3q125_energy_step_matches_oracle(orc, pond, shape, bc):
-    """The staged D3Q125 tile kernel with energy populations (float32)."""
+def test_d3q125_energy_step_matches_oracle(orc, pond, shape, bc, precision):
+    """The staged D3Q125 tile kernel with energy populations (float32: 4^3
+    tiles; float64: 2^3 tiles)."""
     dof, tau = 2, 0.9
     rho, g = smooth_state(shape, 3, seed=5, modes=1, du=0.03)
     f = perturbed_populations(orc, 2, rho, g, seed=5, eps=0.01)
     st = orc.with_energy(orc.State(f, rho, g), 2, dof)
     st.h = st.h * (1 + 0.01 * np.random.default_rng(9).standard_normal(st.h.shape))
     names = {0: "periodic", 1: "clamp", 2: "mirror"}
-    with pond.Solver(lattice="D3Q125", shape=shape, precision="fp32", tau=tau,
+    with pond.Solver(lattice="D3Q125", shape=shape, precision=precision, tau=tau,
                      bc=tuple(names[b] for b in bc), ddf_dof=dof) as s:
         s.set_state(st.rho, st.g, f=st.f)
         s.set_energy(st.h)
@@ -163,7 +165,7 @@ def test_d3q125_energy_step_matches_oracle(orc, pond, shape, bc):
                                       tol_abs=s.params.tol_abs, tol_rel=s.params.tol_rel)
         err = _errors(s, ref)
         d = s.diagnostics()
-    assert all(v <= TOL["fp32"] for v in err.values()), err
+    assert all(v <= TOL[precision] for v in err.values()), err
     assert d["nonconverged"] == 0
     total = np.sum(ref.rho * (np.sum(ref.g[:3] ** 2, axis=0) + (3 + dof) * ref.g[3]))
     assert abs(d["enrg"] - total) <= 1e-6 * abs(total)
@@ -209,5 +211,5 @@ def test_energy_api(orc, pond):
         s.set_state(rho, g)
         with pytest.raises(pond._lib.PondError):
             s.get_energy()
-    with pytest.raises(pond._lib.PondError):  # D3Q125 energy populations run in float32 only
-        pond.Solver(lattice="D3Q125", shape=(4, 4, 4), precision="fp64", ddf_dof=2)
+    with pytest.raises(pond._lib.PondError):  # no energy populations on the D3Q27 WENO5 schemes
+        pond.Solver(lattice="D3Q27", shape=(8, 4, 4), interp=pond.WENO5, ddf_dof=2)
