@@ -768,11 +768,13 @@ def run_configs_full(which, d3q125_size=192, l1_size_d3q125=48):
       2  D3Q27 Taylor-Green 128^3, quadratic, tau 0.51, 2000 steps, float32
          against float64
       3  the batched D1Q5 problems (the benchmark line's batch1d)
-      4  D3Q27 sphere 256^3, cubic, tau 0.52, 1500 steps: float32 plain and
-         learned (pairs from steps 121-150, the network attached from step 151);
-         each against the float64 path over three steps from its final state
-         (a float64 run of the whole 1500 steps at 256^3 takes over half an
-         hour)
+      4  D3Q27 sphere 256^3, cubic, tau 0.52, up to 1500 steps: float32 plain
+         and learned (pairs from steps 121-150, the network attached from
+         step 151), each stopped at its first non-finite check (the
+         rarefaction focusing at the centre drives rho and T towards 0 there)
+         and held against the float64 path over three steps from its last
+         finite checkpoint; and the step by which the float32 and the float64
+         path go non-finite at 128^3
       5  D3Q125 shock + vortex at d3q125_size^3, centred WENO5, inflow/outflow
          in x, 1000 steps, float32; L1 against float64 over ten steps from
          the final state (the float64 path at the reference's tolerance);
@@ -842,27 +844,18 @@ def run_configs_full(which, d3q125_size=192, l1_size_d3q125=48):
         out["batch1d"] = run_batch1d(1000, 4096)
         note("batch done")
     if "4" in which:
-        n, nsteps, spin, l1_steps = 256, 1500, 150, 3
-        mk = lambda prec="fp32": pond.Solver(lattice="D3Q27", shape=(n,) * 3, interp=pond.LAGR4,  # noqa: E731
-                                            precision=prec, tau=TAU, tol_abs=TOL_ABS if prec == "fp32" else None,
-                                            tol_rel=TOL_REL if prec == "fp32" else None)
-        rec = {"workload": f"D3Q27 {n}^3 spherical Riemann problem, tau {TAU}, cubic Lagrange, {nsteps} steps; "
-                           f"L1 against the float64 path over {l1_steps} steps from each run's final state"}
-        note("sphere 256^3: plain float32 run")
+        n, nsteps, spin, l1_steps, chunk = 256, 1500, 150, 3, 25
+        mk = lambda prec="fp32", m=n: pond.Solver(lattice="D3Q27", shape=(m,) * 3, interp=pond.LAGR4,  # noqa: E731
+                                                 precision=prec, tau=TAU,
+                                                 tol_abs=TOL_ABS if prec == "fp32" else None,
+                                                 tol_rel=TOL_REL if prec == "fp32" else None)
+        rec = {"workload": f"D3Q27 {n}^3 spherical Riemann problem, tau {TAU}, cubic Lagrange, up to {nsteps} "
+                           f"steps; the state goes non-finite where the rarefaction focuses at the centre, so each "
+                           f"run stops at the first non-finite check (every {chunk} steps) and its L1 is taken over "
+                           f"{l1_steps} steps from the last finite checkpoint"}
 
-        def l1_window(s):
-            """float32 against float64 over l1_steps steps from s's state (s advances)."""
-            note("float64 window")
-            with mk("fp64") as r:
-                r.copy_state_from(s)
-                d0 = r.diagnostics()
-                r.step(l1_steps)
-                fr = r.fields()
-                dr = _drift(d0, r.diagnostics(), l1_steps)
-                ms64 = r.last_step_ms() / l1_steps
-            s.step(l1_steps)
-            return {"window": f"steps {nsteps + 1}..{nsteps + l1_steps}", **_l1_fields(s.fields(), fr),
-                    "fp64_drift_in_window": dr, "fp64_ms_per_step": ms64}
+        def finite(s):
+            return bool(np.isfinite(s.diagnostics()["mass"]))
 
         def progress(s, label, k, ms):
             d, fl = s.diagnostics(), s.fields()
@@ -871,27 +864,52 @@ def run_configs_full(which, d3q125_size=192, l1_size_d3q125=48):
                  f"nonconverged {d['nonconverged']}, T {fl['T'].min():.4g}..{fl['T'].max():.4g}, max |u| {umax:.4g}, "
                  f"rho {fl['rho'].min():.4g}..{fl['rho'].max():.4g}")
 
-        with mk() as s:
+        def l1_window(snap, k0):
+            """float32 against float64 over l1_steps steps from the snapshot taken after step k0."""
+            note(f"float64 window from step {k0}")
+            with mk("fp64") as r:
+                r.copy_state_from(snap)
+                d0 = r.diagnostics()
+                r.step(l1_steps)
+                fr = r.fields()
+                dr = _drift(d0, r.diagnostics(), l1_steps)
+                ms64 = r.last_step_ms() / l1_steps
+            snap.step(l1_steps)
+            return {"window": f"steps {k0 + 1}..{k0 + l1_steps}", **_l1_fields(snap.fields(), fr),
+                    "fp64_drift_in_window": dr, "fp64_ms_per_step": ms64}
+
+        def run(s, snap, label, k_start, ms0):
+            """Steps s from k_start to nsteps in chunks, keeping the last finite
+            state in snap; returns (steps run, device ms, first non-finite check)."""
+            ms, k, bad = ms0, k_start, None
+            snap.copy_state_from(s)
+            kept = k
+            while k < nsteps:
+                ms += _chunked(s, min(chunk, nsteps - k))
+                k = min(k + chunk, nsteps)
+                progress(s, label, k, ms)
+                if not finite(s):
+                    bad = k
+                    break
+                snap.copy_state_from(s)
+                kept = k
+            return k, ms, bad, kept
+
+        with mk() as s, mk() as snap:
             s.init("sphere", *sphere_params())
             d0 = s.diagnostics()
-            ms, done = 0.0, 0
-            for k0 in range(0, nsteps, 25):
-                ms += _chunked(s, min(25, nsteps - k0))
-                done = min(k0 + 25, nsteps)
-                progress(s, "plain", done, ms)
-                if not np.isfinite(s.diagnostics()["mass"]):
-                    break
+            done, ms, bad, kept = run(s, snap, "plain", 0, 0.0)
             d = s.diagnostics()
-            rec["plain"] = {"steps_run": done, "ms_per_step": ms / done, "MLUPS": n ** 3 / (ms / done) / 1e3,
-                            "drift": _drift(d0, d, done), "niter_mean_last_step": d["niter_mean"],
-                            "nonconverged_last_step": d["nonconverged"]}
-            if done == nsteps:
-                rec["plain"]["l1_vs_fp64"] = l1_window(s)
+            rec["plain"] = {"steps_run": done, "non_finite_by_step": bad, "last_finite_checkpoint": kept,
+                            "ms_per_step": ms / done, "MLUPS": n ** 3 / (ms / done) / 1e3,
+                            "drift_to_checkpoint": _drift(d0, snap.diagnostics(), kept),
+                            "niter_mean_last_step": d["niter_mean"], "nonconverged_last_step": d["nonconverged"],
+                            "l1_vs_fp64": l1_window(snap, kept)}
         note("sphere plain done")
         cap = 4_000_000
         X = torch.empty((cap, 39), dtype=torch.float32, device="cuda")
         Y = torch.empty((cap, 4), dtype=torch.float32, device="cuda")
-        with mk() as s:
+        with mk() as s, mk() as snap:
             s.init("sphere", *sphere_params())
             d0 = s.diagnostics()
             rows = 0
@@ -907,25 +925,34 @@ def run_configs_full(which, d3q125_size=192, l1_size_d3q125=48):
             net.train(X[:rows], Y[:rows], steps=10000, batch=8192, lr=2e-3)
             gate, _ = calibrate_gate(net, X[:rows], Y[:rows])
             attach(s, net, gate=gate)
-            ms_l, done = 0.0, spin
-            for k0 in range(spin, nsteps, 150):
-                ms_l += _chunked(s, min(150, nsteps - k0))
-                done = min(k0 + 150, nsteps)
-                progress(s, "learned", done, ms + ms_l)
-                if not np.isfinite(s.diagnostics()["mass"]):
-                    break
+            done, ms_all, bad, kept = run(s, snap, "learned", spin, ms)
             d = s.diagnostics()
             attach(s, None)
             net.close()
-            rec["learned"] = {"steps_run": done, "ms_per_step": (ms + ms_l) / done,
-                              "MLUPS": n ** 3 / ((ms + ms_l) / done) / 1e3,
-                              "ms_per_step_after_attach": ms_l / (done - spin),
-                              "MLUPS_after_attach": n ** 3 / (ms_l / (done - spin)) / 1e3,
-                              "drift": _drift(d0, d, done), "niter_mean_last_step": d["niter_mean"],
-                              "nonconverged_last_step": d["nonconverged"]}
-            if done == nsteps:
-                rec["learned"]["l1_vs_fp64"] = l1_window(s)
+            rec["learned"] = {"steps_run": done, "non_finite_by_step": bad, "last_finite_checkpoint": kept,
+                              "ms_per_step": ms_all / done, "MLUPS": n ** 3 / (ms_all / done) / 1e3,
+                              "MLUPS_after_attach": n ** 3 / ((ms_all - ms) / (done - spin)) / 1e3,
+                              "drift_to_checkpoint": _drift(d0, snap.diagnostics(), kept),
+                              "niter_mean_last_step": d["niter_mean"], "nonconverged_last_step": d["nonconverged"],
+                              "l1_vs_fp64": l1_window(snap, kept)}
         note("sphere learned done")
+        # the same problem at 128^3 in both precisions: does the float64 path go non-finite too?
+        m = n // 2
+        div = {}
+        for prec in ("fp32", "fp64"):
+            with mk(prec, m) as s:
+                s.init("sphere", *sphere_params())
+                k, first = 0, None
+                while k < nsteps // 2:
+                    s.step(min(chunk // 2, nsteps // 2 - k))
+                    k = min(k + chunk // 2, nsteps // 2)
+                    if not finite(s):
+                        first = k
+                        break
+                div[prec] = {"non_finite_by_step": first, "steps_run": k, "check_every": chunk // 2,
+                             "tolerance": [TOL_ABS, TOL_REL] if prec == "fp32" else [1e-12, 1e-10]}
+            note(f"sphere {m}^3 {prec}: non-finite by step {first}")
+        rec[f"divergence_{m}cube"] = div
         out["sphere_d3q27_256"] = rec
     if "5" in which:
         m, nsteps, l1_steps = d3q125_size, 1000, 10
