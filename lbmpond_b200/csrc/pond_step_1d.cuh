@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(128) pull_1d_scheme_kernel(StepArgs<R> a) {
             hi = max(hi, org[k][m] + 3);
           }
         } else {
-          const double crd = double(x) - vk[k];
+          const double crd = held_coordinate(double(x) - vk[k]);
           base[k] = (int)(floor(crd + 0.5) - 2);
           lo = min(lo, base[k]);
           hi = max(hi, base[k] + 4);
@@ -112,7 +112,9 @@ __global__ void __launch_bounds__(128) pull_1d_scheme_kernel(StepArgs<R> a) {
 #pragma unroll
         for (int m = 0; m < NS; m++) acc[k][m] = R(0);
       ns.work += (unsigned long long)(hi - lo + 1);
-      for (int p = lo; p <= hi; p++) {
+      // the positions inside some window, in increasing order (gaps skipped)
+      for (int p = lo; p <= hi;
+           p = SCHEME == POND_TVD ? windows_next<Q * NS, 4, 1>(&org[0][0], p) : windows_next<Q, 5, 1>(base, p)) {
         bool rv[3] = {false, false, false};
         const int rx = resolve_axis(p, a.nx, a.bc[0], rv[0]);
         R fn[Q], s[3], r[3];

@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(128) pull_1d_energy_kernel(StepArgs<R> a) {
             hi = max(hi, org[k][m] + 3);
           }
         } else {
-          const double crd = double(x) - vk[k];
+          const double crd = held_coordinate(double(x) - vk[k]);
           wb[k] = (int)(floor(crd + 0.5) - 2);
           lo = min(lo, wb[k]);
           hi = max(hi, wb[k] + 4);
@@ -91,7 +91,10 @@ __global__ void __launch_bounds__(128) pull_1d_energy_kernel(StepArgs<R> a) {
 #pragma unroll
         for (int m = 0; m < NS; m++) { accf[k][m] = R(0); acch[k][m] = R(0); }
       ns.work += (unsigned long long)(hi - lo + 1);
-      for (int p = lo; p <= hi; p++) {
+      // the positions inside some window, in increasing order (gaps skipped)
+      for (int p = lo; p <= hi;
+           p = kLagr ? windows_next<Q, NL, NS>(&org[0][0], p)
+                     : SCHEME == POND_TVD ? windows_next<Q * NS, 4, 1>(&org[0][0], p) : windows_next<Q, 5, 1>(wb, p)) {
         bool rv[3] = {false, false, false};
         const int rx = resolve_axis(p, a.nx, a.bc[0], rv[0]);
         R fn[Q], s[3], r[3];

@@ -70,6 +70,26 @@ template <int N, int Q1> __device__ __forceinline__ int window_next(const int or
   }
   return in ? q : nxt;
 }
+// The same walk over NW windows of LEN positions whose starts lie STRIDE
+// ints apart (the 1D schemes' per-population windows).
+template <int NW, int LEN, int STRIDE> __device__ __forceinline__ int windows_next(const int* start, int p) {
+  const int q = p + 1;
+  bool in = false;
+  int nxt = 0x7fffffff;
+#pragma unroll
+  for (int w = 0; w < NW; w++) {
+    const int st = start[w * STRIDE];
+    in = in || (q - st >= 0 && q - st < LEN);
+    nxt = st > p ? min(nxt, st) : nxt;
+  }
+  return in ? q : nxt;
+}
+// a departure coordinate held within +-2^29 (a NaN stays NaN), for windows
+// placed without window_origin
+__device__ __forceinline__ double held_coordinate(double c) {
+  return fabs(c) > 536870912.0 ? copysign(536870912.0, c) : c;
+}
+
 // number of positions the walk visits
 template <int N, int Q1> __device__ __forceinline__ int window_positions(const int org[Q1]) {
   int n = 0;
